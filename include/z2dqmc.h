@@ -1,0 +1,145 @@
+/*
+ * z2dqmc.h -- C ABI of the B200 (sm_100a) DQMC library for spinful fermions
+ * coupled to a Z2 lattice gauge field.
+ *
+ * The library replaces the hot path of the Fortran program z2_gauge.out
+ * (SONY932/z2_gauge_zfy).  Each entry point names the reference module
+ * procedure it stands in for (file:line relative to the reference root).
+ * The reference keeps its state in module globals (src/model.f90:10-13,
+ * src/local_sweep.f90:27-29, src/stabilization.f90:10-17); here that state
+ * lives in an opaque handle that owns the device memory of a batch of
+ * independent Markov chains (one chain = one MPI rank of the reference).
+ *
+ * Conventions
+ *  - Every call returns an int status (z2_status); z2_last_error() gives text.
+ *  - All matrices are real float64, column-major N x N, N = Nlx*Nly (the
+ *    reference stores complex(kind=8) but every entry is real).
+ *  - sigma is float64 (+1/-1) laid out as the Fortran array sigma(2*N, Ltrot).
+ *  - Time-slice numbers nt follow the reference (1..Ltrot, 0 for the
+ *    boundary), bond numbers are 0-based (reference bond ii -> ii-1).
+ *  - Calls are synchronous on the handle's stream; the library copies into
+ *    and out of caller-owned host buffers.  A handle is not thread-safe.
+ */
+#ifndef Z2DQMC_H
+#define Z2DQMC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum z2_status {
+  Z2_OK = 0,
+  Z2_ERR_ARG = 1,        /* invalid argument (the reference would `stop`) */
+  Z2_ERR_CUDA = 2,       /* a CUDA runtime call failed */
+  Z2_ERR_NONFINITE = 3,  /* NaN/Inf in a Green's function or a D factor */
+  Z2_ERR_STATE = 4,      /* call out of order (e.g. sweep before pre) */
+  Z2_ERR_NOMEM = 5,      /* device allocation failed */
+  Z2_ERR_TIMEOUT = 6     /* a bounded device-side wait gave up */
+};
+
+/* Number of doubles returned by z2_get_obs_equal: flux_avg, chi_flux,
+ * pair_sc_q0, cdw_pi, cdw_shift, cdw_ratio, density (the fields written by
+ * Obs_equal_ave, src/obser_equal.f90:50-71). */
+#define Z2_NOBS_EQ 7
+/* Number of time-displaced correlators (src/obser_tau.f90:9-10), in the
+ * order spin, single, pair_d, pair_s, charge_d, charge_s, curxx. */
+#define Z2_NOBS_TAU 7
+/* Number of doubles returned by z2_get_stats: acc (sum over bins of the
+ * accepted fraction, AccCounter%acc), Xmaxm, Xmeanm (Propagator drift,
+ * src/process_matrix.f90:10), Xmaxm(1:3), Xmeanm(1:3) of the time-displaced
+ * chain (src/process_matrix.f90:20), accepted, proposed (this bin),
+ * rng draws so far, nobs, nobst. */
+#define Z2_NSTATS 14
+
+/* One chain's parameters: the lines of paramC_sets.txt that the hot path
+ * reads (src/calc_basic.f90:52-62) plus this chain's seed (seeds.txt). */
+typedef struct z2_chain_params {
+  double RT, J, h, mu, Q;       /* line 1 */
+  int32_t Nlx, Nly, Ltrot;      /* line 2 */
+  double beta;                  /* line 2 */
+  int32_t Nwrap;                /* line 4 */
+  int32_t absolute;             /* line 8: initial sigma mode 1..5 */
+  int32_t seed;                 /* seeds.txt row of this chain */
+  const double *rt_bond;        /* optional [2N] per-bond hopping, NULL = RT */
+} z2_chain_params;
+
+typedef struct z2_options {
+  int32_t delay_k;   /* accepted flips queued before a rank-2k flush; 0 = tuned */
+  int32_t record;    /* 1: keep decisions and ratios of each half-sweep */
+  int32_t device;    /* CUDA device ordinal */
+  int32_t tau;       /* 1: allocate the time-displaced chain (is_tau) */
+} z2_options;
+
+typedef struct z2_handle z2_handle;
+
+/* ---- life cycle: Model_init + Prop/WrapList make + Stabilize_init
+ *      (src/model.f90:16-36, src/process_matrix.f90:46-112,
+ *       src/stabilization.f90:20-32); the initial sigma follows conf_set +
+ *      conf_transfer (src/fields.f90:311-507) from each chain's seed. ---- */
+int z2_create(z2_handle **out, const z2_chain_params *params, int32_t nchains,
+              const z2_options *opt);
+int z2_destroy(z2_handle *h);
+const char *z2_last_error(const z2_handle *h);
+int z2_chain_dims(const z2_handle *h, int32_t chain, int32_t *N, int32_t *Ltrot,
+                  int32_t *Nst);
+
+/* ---- configuration I/O: conf_in / conf_out (src/fields.f90:214-309,
+ *      509-557).  iseed is the ranf state that continues the chain. ---- */
+int z2_set_config(z2_handle *h, int32_t chain, const double *sigma, int32_t iseed);
+int z2_get_config(const z2_handle *h, int32_t chain, double *sigma, int32_t *iseed);
+
+/* ---- Local_sweep%pre (src/local_sweep.f90:87-104) on every chain ---- */
+int z2_pre(z2_handle *h);
+/* ---- Local_sweep%sweep (src/local_sweep.f90:152-195): one bin of nsweep
+ *      (sweep_L, sweep_R) pairs on every chain; toggle = is_tau for this
+ *      bin (runs Dyn%reset/sweep_R, src/dynamics.f90:41-62).  The whole bin
+ *      of every chain runs in one persistent launch. ---- */
+int z2_sweep(z2_handle *h, int32_t nsweep, int32_t toggle);
+/* Same as z2_sweep, also returning the device time of the launch (ms). */
+int z2_sweep_timed(z2_handle *h, int32_t nsweep, int32_t toggle, float *ms);
+
+/* ---- readback ---- */
+int z2_get_green(const z2_handle *h, int32_t chain, double *G);
+int z2_get_obs_equal(const z2_handle *h, int32_t chain, double out[Z2_NOBS_EQ]);
+/* out: Z2_NOBS_TAU arrays of (N, Ltrot) column-major, real parts (the
+ * imaginary parts of ObserTau are identically zero for real G). */
+int z2_get_obs_tau(const z2_handle *h, int32_t chain, double *out);
+int z2_get_stats(const z2_handle *h, int32_t chain, double out[Z2_NSTATS]);
+/* Replay: use r[0..n) instead of ranf for the next n proposals (n = 0
+ * restores ranf).  Decisions/ratios of the last half-sweeps, in the order
+ * (half-sweep L then R, slice nt = 1..Ltrot, bond 0..2N-1). */
+int z2_set_replay(z2_handle *h, int32_t chain, const double *r, size_t n);
+int z2_get_decisions(const z2_handle *h, int32_t chain, uint8_t *dec,
+                     double *ratios, size_t n);
+
+/* ---- adjoint (no reference routine): log|det(1 + B_Ltrot...B_1)| of one
+ *      spin sector and its gradient wrt the 2N per-bond hopping amplitudes
+ *      and mu, at the chain's current sigma. ---- */
+int z2_logdet_grad(z2_handle *h, int32_t chain, double *logdet,
+                   double *dlogdet_dt, double *dlogdet_dmu);
+
+/* ---- module-level mirrors on single matrices (host buffers) ----
+ * OperatorKin%mmult_R / mmult_L (src/operator_kin.f90:61-86, 122-145):
+ *   M <- B_nt^nflag M   /   M <- M B_nt^nflag, with the chain's sigma. */
+int z2_opk_mmult_R(z2_handle *h, int32_t chain, double *M, int32_t nt, int32_t nflag);
+int z2_opk_mmult_L(z2_handle *h, int32_t chain, double *M, int32_t nt, int32_t nflag);
+/* stab_UR / stab_UL (src/stabilization.f90:70-120): in-place U, D, V. */
+int z2_stab_UR(z2_handle *h, int32_t chain, double *U, double *D, double *V);
+int z2_stab_UL(z2_handle *h, int32_t chain, double *U, double *D, double *V);
+/* stab_green (src/stabilization.f90:122-200). */
+int z2_stab_green(z2_handle *h, int32_t chain, const double *UR, const double *DR,
+                  const double *VR, const double *UL, const double *DL,
+                  const double *VL, int32_t nt, double *G);
+/* stab_green_big (src/stabilization.f90:202-264). */
+int z2_stab_green_big(z2_handle *h, int32_t chain, const double *UR,
+                      const double *DR, const double *VR, const double *UL,
+                      const double *DL, const double *VL, double *G00,
+                      double *G0t, double *Gt0, double *Gtt);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* Z2DQMC_H */

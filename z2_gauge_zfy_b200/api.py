@@ -1,0 +1,242 @@
+"""Host-side mirror of the reference's module interfaces for the DQMC hot path.
+
+``Z2Batch`` owns a batch of independent Markov chains on one GPU (the
+reference runs one chain per MPI rank).  Its methods mirror
+``LocalSweep%pre`` / ``%sweep`` (src/local_sweep.f90:87-195), the readback of
+``ObserEqual`` / ``ObserTau`` (src/obser_equal.f90, src/obser_tau.f90) and the
+drift statistics of ``Propagator`` / ``PropGreen`` (src/process_matrix.f90).
+The module-level functions mirror ``OperatorKin%mmult_R/L``
+(src/operator_kin.f90:61-145) and the ``stab_*`` routines of
+src/stabilization.f90 on single matrices.
+
+Matrices are numpy arrays in natural (row, column) indexing; they are
+converted to the library's column-major layout at the boundary.  Errors raise
+``Z2Error`` (the reference would print and ``stop``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _ffi
+from ._ffi import ChainParams, Options, Z2Error, dptr, fmat
+
+OBS_EQ_NAMES = ("flux_avg", "chi_flux", "pair_sc_q0", "cdw_pi", "cdw_shift", "cdw_ratio",
+                "density")
+OBS_TAU_NAMES = ("spin", "single", "pair_d", "pair_s", "charge_d", "charge_s", "curxx")
+STAT_NAMES = ("acc", "Xmaxm", "Xmeanm", "Xmaxm_tau0", "Xmaxm_tau1", "Xmaxm_tau2",
+              "Xmeanm_tau0", "Xmeanm_tau1", "Xmeanm_tau2", "accepted", "proposed", "draws",
+              "nobs", "nobst")
+
+
+@dataclass
+class Chain:
+    """Parameters of one chain: the hot-path lines of paramC_sets.txt
+    (src/calc_basic.f90:52-62) and this chain's row of seeds.txt."""
+    RT: float = 1.0
+    J: float = 0.5
+    h: float = 0.5
+    mu: float = 0.0
+    Q: float = 1.0
+    Nlx: int = 4
+    Nly: int = 4
+    Ltrot: int = 40
+    beta: float = 4.0
+    Nwrap: int = 10
+    absolute: int = 1
+    seed: int = 12345
+    rt_bond: np.ndarray | None = None
+
+    @property
+    def N(self):
+        return self.Nlx * self.Nly
+
+
+def _check(lib, h, code):
+    if code != 0:
+        msg = lib.z2_last_error(h)
+        raise Z2Error(code, msg.decode() if msg else "")
+
+
+class Z2Batch:
+    """A batch of chains resident on one GPU (``z2_create``)."""
+
+    def __init__(self, chains, delay_k: int = 0, record: bool = False, device: int = 0,
+                 tau: bool = False):
+        self.lib = _ffi.load()
+        self.chains = list(chains)
+        n = len(self.chains)
+        arr = (ChainParams * n)()
+        self._rt_keep = []
+        for i, ch in enumerate(self.chains):
+            p = arr[i]
+            p.RT, p.J, p.h, p.mu, p.Q = ch.RT, ch.J, ch.h, ch.mu, ch.Q
+            p.Nlx, p.Nly, p.Ltrot, p.beta = ch.Nlx, ch.Nly, ch.Ltrot, ch.beta
+            p.Nwrap, p.absolute, p.seed = ch.Nwrap, ch.absolute, ch.seed
+            if ch.rt_bond is not None:
+                rb = np.ascontiguousarray(ch.rt_bond, dtype=np.float64)
+                assert rb.shape == (2 * ch.N,)
+                self._rt_keep.append(rb)
+                p.rt_bond = dptr(rb)
+            else:
+                p.rt_bond = None
+        opt = Options(delay_k, 1 if record else 0, device, 1 if tau else 0)
+        h = C.c_void_p()
+        code = self.lib.z2_create(C.byref(h), arr, n, C.byref(opt))
+        self.h = h
+        if code != 0:
+            msg = self.lib.z2_last_error(h)
+            self.lib.z2_destroy(h)
+            self.h = None
+            raise Z2Error(code, msg.decode() if msg else "")
+
+    # -- life cycle ---------------------------------------------------------
+    def close(self):
+        if self.h is not None:
+            self.lib.z2_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _c(self, code):
+        _check(self.lib, self.h, code)
+
+    # -- LocalSweep ----------------------------------------------------------
+    def pre(self):
+        """``Local_sweep_pre`` on every chain."""
+        self._c(self.lib.z2_pre(self.h))
+
+    def sweep(self, nsweep: int = 1, toggle: bool = False) -> None:
+        """``Local_sweep`` (one bin of ``nsweep`` L+R sweep pairs) on every chain."""
+        self._c(self.lib.z2_sweep(self.h, nsweep, 1 if toggle else 0))
+
+    def sweep_timed(self, nsweep: int = 1, toggle: bool = False) -> float:
+        """Like ``sweep``; returns the device time of the launch in ms."""
+        ms = C.c_float()
+        self._c(self.lib.z2_sweep_timed(self.h, nsweep, 1 if toggle else 0, C.byref(ms)))
+        return float(ms.value)
+
+    # -- configuration -------------------------------------------------------
+    def dims(self, chain: int):
+        N, L, S = C.c_int32(), C.c_int32(), C.c_int32()
+        self._c(self.lib.z2_chain_dims(self.h, chain, C.byref(N), C.byref(L), C.byref(S)))
+        return N.value, L.value, S.value
+
+    def get_config(self, chain: int):
+        """sigma(2N, Ltrot) and the ranf state (``conf_out``)."""
+        N, L, _ = self.dims(chain)
+        buf = np.empty(2 * N * L)
+        seed = C.c_int32()
+        self._c(self.lib.z2_get_config(self.h, chain, dptr(buf), C.byref(seed)))
+        return buf.reshape(L, 2 * N).T.copy(), seed.value
+
+    def set_config(self, chain: int, sigma, iseed: int):
+        """Load sigma(2N, Ltrot) and the ranf state (``conf_in``)."""
+        s = fmat(sigma).ravel()
+        self._c(self.lib.z2_set_config(self.h, chain, dptr(s), int(iseed)))
+
+    # -- readback ------------------------------------------------------------
+    def green(self, chain: int) -> np.ndarray:
+        N = self.dims(chain)[0]
+        buf = np.empty(N * N)
+        self._c(self.lib.z2_get_green(self.h, chain, dptr(buf)))
+        return buf.reshape(N, N).T.copy()
+
+    def obs_equal(self, chain: int) -> dict:
+        buf = np.empty(_ffi.Z2_NOBS_EQ)
+        self._c(self.lib.z2_get_obs_equal(self.h, chain, dptr(buf)))
+        return dict(zip(OBS_EQ_NAMES, buf.tolist()))
+
+    def obs_tau(self, chain: int) -> dict:
+        N, L, _ = self.dims(chain)
+        buf = np.empty(7 * N * L)
+        self._c(self.lib.z2_get_obs_tau(self.h, chain, dptr(buf)))
+        a = buf.reshape(7, L, N)
+        return {k: a[q].T.copy() for q, k in enumerate(OBS_TAU_NAMES)}
+
+    def stats(self, chain: int) -> dict:
+        buf = np.empty(_ffi.Z2_NSTATS)
+        self._c(self.lib.z2_get_stats(self.h, chain, dptr(buf)))
+        return dict(zip(STAT_NAMES, buf.tolist()))
+
+    def set_replay(self, chain: int, values):
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        self._c(self.lib.z2_set_replay(self.h, chain, dptr(v) if v.size else None, v.size))
+
+    def decisions(self, chain: int):
+        """Decisions and ratios of the last half-sweeps as arrays [2, Ltrot, 2N]
+        (L half-sweep then R)."""
+        N, L, _ = self.dims(chain)
+        n = 2 * L * 2 * N
+        dec = np.empty(n, dtype=np.uint8)
+        rat = np.empty(n)
+        self._c(self.lib.z2_get_decisions(self.h, chain, dec.ctypes.data_as(C.POINTER(C.c_uint8)),
+                                          dptr(rat), n))
+        return dec.reshape(2, L, 2 * N), rat.reshape(2, L, 2 * N)
+
+    def logdet_grad(self, chain: int):
+        """log|det(1+B)| of one spin sector, d/dt_b (2N) and d/dmu."""
+        N = self.dims(chain)[0]
+        ld, dmu = C.c_double(), C.c_double()
+        g = np.empty(2 * N)
+        self._c(self.lib.z2_logdet_grad(self.h, chain, C.byref(ld), dptr(g), C.byref(dmu)))
+        return ld.value, g, dmu.value
+
+    # -- module-level mirrors --------------------------------------------------
+    def opk_mmult_R(self, chain: int, M, nt: int, nflag: int) -> np.ndarray:
+        """B_nt^nflag M (``OperatorKin%mmult_R``), nt = 1..Ltrot."""
+        b = fmat(M).ravel()
+        self._c(self.lib.z2_opk_mmult_R(self.h, chain, dptr(b), nt, nflag))
+        n = int(round(np.sqrt(b.size)))
+        return b.reshape(n, n).T.copy()
+
+    def opk_mmult_L(self, chain: int, M, nt: int, nflag: int) -> np.ndarray:
+        """M B_nt^nflag (``OperatorKin%mmult_L``)."""
+        b = fmat(M).ravel()
+        self._c(self.lib.z2_opk_mmult_L(self.h, chain, dptr(b), nt, nflag))
+        n = int(round(np.sqrt(b.size)))
+        return b.reshape(n, n).T.copy()
+
+    def _stab_u(self, fn, chain, U, D, V):
+        n = U.shape[0]
+        u, v = fmat(U).ravel(), fmat(V).ravel()
+        d = np.ascontiguousarray(D, dtype=np.float64).copy()
+        self._c(fn(self.h, chain, dptr(u), dptr(d), dptr(v)))
+        return u.reshape(n, n).T.copy(), d, v.reshape(n, n).T.copy()
+
+    def stab_UR(self, chain, U, D, V):
+        """``stab_UR``: returns the new (UR, DR, VR)."""
+        return self._stab_u(self.lib.z2_stab_UR, chain, U, D, V)
+
+    def stab_UL(self, chain, U, D, V):
+        """``stab_UL``: returns the new (UL, DL, VL)."""
+        return self._stab_u(self.lib.z2_stab_UL, chain, U, D, V)
+
+    def stab_green(self, chain, UR, DR, VR, UL, DL, VL, nt: int) -> np.ndarray:
+        n = UR.shape[0]
+        g = np.empty(n * n)
+        args = [fmat(UR).ravel(), np.ascontiguousarray(DR, dtype=np.float64), fmat(VR).ravel(),
+                fmat(UL).ravel(), np.ascontiguousarray(DL, dtype=np.float64), fmat(VL).ravel()]
+        self._c(self.lib.z2_stab_green(self.h, chain, *[dptr(a) for a in args], nt, dptr(g)))
+        return g.reshape(n, n).T.copy()
+
+    def stab_green_big(self, chain, UR, DR, VR, UL, DL, VL):
+        n = UR.shape[0]
+        outs = [np.empty(n * n) for _ in range(4)]
+        args = [fmat(UR).ravel(), np.ascontiguousarray(DR, dtype=np.float64), fmat(VR).ravel(),
+                fmat(UL).ravel(), np.ascontiguousarray(DL, dtype=np.float64), fmat(VL).ravel()]
+        self._c(self.lib.z2_stab_green_big(self.h, chain, *[dptr(a) for a in args],
+                                           *[dptr(o) for o in outs]))
+        return tuple(o.reshape(n, n).T.copy() for o in outs)

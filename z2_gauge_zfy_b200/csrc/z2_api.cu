@@ -1,0 +1,890 @@
+// z2_api.cu -- kernels and the C ABI (include/z2dqmc.h) of the B200 DQMC
+// library.  Build: nvcc -gencode arch=compute_100a,code=sm_100a -O3 -shared.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/z2dqmc.h"
+#include "z2_drivers.cuh"
+
+enum { OP_PRE = 1, OP_SWEEP = 2, OP_LOGDET = 3 };
+enum { U_MMULT_R = 1, U_MMULT_L, U_STAB_UR, U_STAB_UL, U_STAB_GREEN, U_STAB_GREEN_BIG };
+
+struct UnitArgs {
+  double *M;                      // mmult: in/out
+  double *U, *D, *V;              // stab_U: in/out (U = UR or UL^T)
+  const double *UR, *DR, *VR, *ULT, *DL, *VL;
+  double *G, *G0t, *Gt0, *Gtt;    // outputs
+  int nt, nflag;
+};
+
+// ---------------------------------------------------------------------------
+// Kernels
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void load_desc(ChainDesc &sc, const ChainDesc *g) {
+  const long long *src = (const long long *)g;
+  long long *dst = (long long *)&sc;
+  for (int i = threadIdx.x; i < (int)(sizeof(ChainDesc) / 8); i += Z2_NT) dst[i] = src[i];
+  __syncthreads();
+}
+
+// Persistent launch: every CTA pulls chains from a work queue (ordered by
+// decreasing cost) and runs the whole operation of that chain.
+__global__ void __launch_bounds__(Z2_NT, 1)
+z2_chain_kernel(const ChainDesc *descs, const int *order, int nchains, int *queue, int op,
+                int nsweep, int toggle, unsigned smem_bytes) {
+  extern __shared__ __align__(16) unsigned char z2_smem[];
+  __shared__ ChainDesc sc;
+  __shared__ int s_idx;
+  for (;;) {
+    if (threadIdx.x == 0) s_idx = atomicAdd(queue, 1);
+    __syncthreads();
+    const int idx = s_idx;
+    if (idx >= nchains) break;
+    load_desc(sc, descs + order[idx]);
+    Smem s = make_smem(sc, z2_smem, smem_bytes);
+    if (op == OP_PRE) {
+      for (int i = threadIdx.x; i < 2 * sc.nb; i += Z2_NT) s.bond[i] = sc.bonds[i];
+      __syncthreads();
+      chain_pre(sc, s);
+    } else if (op == OP_SWEEP) {
+      chain_sweep(sc, s, nsweep, toggle != 0, sc.hzero ? 1.0 : 0.0);
+    } else if (op == OP_LOGDET) {
+      chain_logdet_grad(sc, s);
+    }
+    __syncthreads();
+  }
+}
+
+// Module-level mirrors on single matrices, one CTA.
+__global__ void __launch_bounds__(Z2_NT, 1)
+z2_unit_kernel(const ChainDesc *desc, int op, UnitArgs a, unsigned smem_bytes) {
+  extern __shared__ __align__(16) unsigned char z2_smem[];
+  __shared__ ChainDesc sc;
+  load_desc(sc, desc);
+  Smem s = make_smem(sc, z2_smem, smem_bytes);
+  const int N = sc.N;
+  if (op == U_MMULT_R || op == U_MMULT_L) {
+    build_table(sc, s, a.nt);
+    if (op == U_MMULT_R) kin_global(sc, s, a.M, a.nflag, 0);
+    else kin_global(sc, s, a.M, 0, a.nflag);
+  } else if (op == U_STAB_UR || op == U_STAB_UL) {
+    int lda; double *A = qr_matrix(sc, s, lda);
+    blk_copy(A, lda, a.U, N, N, N);
+    dev_stab_U(s, N, A, lda, a.U, a.D, a.V, sc.W0, op == U_STAB_UL);
+  } else if (op == U_STAB_GREEN) {
+    int lda; double *A = qr_matrix(sc, s, lda);
+    dev_stab_green(s, N, a.nt, sc.Ltrot, a.UR, a.DR, a.VR, a.ULT, a.DL, a.VL, A, lda, sc.W1,
+                   sc.W2, sc.W0, a.G);
+  } else if (op == U_STAB_GREEN_BIG) {
+    dev_stab_green_big(s, N, a.UR, a.DR, a.VR, a.ULT, a.DL, a.VL, sc.W0, sc.W1, sc.W2, sc.W3,
+                       sc.B0, sc.B1, sc.B2, sc.B3);
+    green_big_extract(N, sc.B3, a.G, a.G0t, a.Gt0, a.Gtt);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+namespace {
+
+const double kZero = 1.0e-10;      // src/calc_basic.f90:5
+const double kUpbound = 1.0e200;   // src/calc_basic.f90:7
+const int kSmemMax = 227 * 1024 - 2048;
+const int kGemmTile = 2 * Z2_GEMM_TK * (Z2_GEMM_TM + 1);
+
+int npbc(int nr, int L) { return nr < 1 ? nr + L : (nr > L ? nr - L : nr); }
+
+// ranf (lib/package_of_matrix/Ran/ran_imada.f:55-68): iq*IP mod 2^31.
+double ranf_host(uint32_t &iq) {
+  iq = (uint32_t)(((uint64_t)iq * 48828125ull) & 0x7fffffffull);
+  return (double)iq / 2147483648.0;
+}
+uint32_t fold_seed(int32_t seed) {
+  // a negative Fortran seed behaves like seed mod 2^31 after the first draw;
+  // keep the 32-bit pattern and let ranf_host reduce it.
+  return (uint32_t)seed;
+}
+
+struct HostLattice {
+  int Lx, Ly, N;
+  std::vector<int> bonds, groups, bbonds, plaq, xy, nbx;
+  std::vector<int> inv_n, inv_bond;
+  bool ok = true;
+  HostLattice(int lx, int ly) : Lx(lx), Ly(ly), N(lx * ly) {
+    // n_list / bond_list (src/lattice.f90:31-60)
+    inv_n.assign((Lx + 1) * (Ly + 1), 0);
+    xy.assign(2 * N, 0);
+    for (int ny = 1, nc = 0; ny <= Ly; ++ny)
+      for (int nx = 1; nx <= Lx; ++nx, ++nc) { xy[2 * nc] = nx; xy[2 * nc + 1] = ny; inv_n[nx + ny * (Lx + 1)] = nc; }
+    auto site = [&](int x, int y) { return inv_n[x + y * (Lx + 1)]; };
+    bonds.assign(4 * N, 0);
+    inv_bond.assign(N * N, -1);
+    for (int ny = 1, nc = 0; ny <= Ly; ++ny)
+      for (int nx = 1; nx <= Lx; ++nx) {
+        int ii = site(nx, ny);
+        int ix = site(npbc(nx + 1, Lx), ny);
+        bonds[2 * nc] = ii; bonds[2 * nc + 1] = ix; inv_bond[ii * N + ix] = nc; ++nc;
+        int iy = site(nx, npbc(ny + 1, Ly));
+        bonds[2 * nc] = ii; bonds[2 * nc + 1] = iy; inv_bond[ii * N + iy] = nc; ++nc;
+      }
+    // checkerboard groups (src/lattice.f90:72-102)
+    std::vector<int> g[4];
+    for (int nc = 0; nc < 2 * N; ++nc) {
+      int ii = bonds[2 * nc], jj = bonds[2 * nc + 1];
+      int ixc = xy[2 * ii], iyc = xy[2 * ii + 1], jxc = xy[2 * jj], jyc = xy[2 * jj + 1];
+      if (npbc(ixc + 1, Lx) == jxc) g[(ixc % 2 == 0) ? 0 : 1].push_back(nc);
+      else if (npbc(iyc + 1, Ly) == jyc) g[(iyc % 2 == 0) ? 2 : 3].push_back(nc);
+    }
+    for (int q = 0; q < 4; ++q) {
+      if ((int)g[q].size() != N / 2) ok = false;
+      groups.insert(groups.end(), g[q].begin(), g[q].end());
+    }
+    // plaquette partners (src/lattice.f90:104-141)
+    bbonds.assign(6 * 2 * N, 0);
+    auto ib = [&](int a, int b) { return inv_bond[a * N + b]; };
+    for (int nc = 0; nc < 2 * N; ++nc) {
+      int ii = bonds[2 * nc], jj = bonds[2 * nc + 1];
+      int ixc = xy[2 * ii], iyc = xy[2 * ii + 1], jxc = xy[2 * jj], jyc = xy[2 * jj + 1];
+      int *o = &bbonds[6 * nc];
+      if (npbc(ixc + 1, Lx) == jxc) {
+        int nx = site(ixc, npbc(iyc + 1, Ly)); o[0] = ib(ii, nx);
+        int ny = site(jxc, npbc(jyc + 1, Ly)); o[1] = ib(nx, ny); o[2] = ib(jj, ny);
+        nx = site(ixc, npbc(iyc - 1, Ly)); o[3] = ib(nx, ii);
+        ny = site(jxc, npbc(jyc - 1, Ly)); o[4] = ib(nx, ny); o[5] = ib(ny, jj);
+      } else {
+        int nx = site(npbc(jxc - 1, Lx), jyc); o[0] = ib(nx, jj);
+        int ny = site(npbc(ixc - 1, Lx), iyc); o[1] = ib(ny, nx); o[2] = ib(ny, ii);
+        nx = site(npbc(jxc + 1, Lx), jyc); o[3] = ib(jj, nx);
+        ny = site(npbc(ixc + 1, Lx), iyc); o[4] = ib(ny, nx); o[5] = ib(ii, ny);
+      }
+    }
+    // plaquettes of Obs_equal_calc (src/obser_equal.f90:84-96), +x neighbours
+    plaq.assign(4 * N, 0);
+    nbx.assign(N, 0);
+    for (int s = 0; s < N; ++s) {
+      int x = xy[2 * s], y = xy[2 * s + 1];
+      int right = site(npbc(x + 1, Lx), y), up = site(x, npbc(y + 1, Ly));
+      int diag = site(npbc(xy[2 * up] + 1, Lx), xy[2 * up + 1]);
+      int rup = site(xy[2 * right], npbc(xy[2 * right + 1] + 1, Ly));
+      plaq[4 * s] = ib(s, right); plaq[4 * s + 1] = ib(right, rup);
+      plaq[4 * s + 2] = ib(up, diag); plaq[4 * s + 3] = ib(s, up);
+      nbx[s] = right;
+    }
+  }
+};
+
+struct ChainHost {
+  z2_chain_params p;
+  int N, Ltrot, Nst, nb;
+  double dtau;
+  std::vector<double> rt;
+  std::vector<signed char> sigma0;   // initial configuration
+  uint32_t iseed0;
+  ChainDesc d;                       // with device pointers
+  size_t bytes = 0;
+  char *base = nullptr;              // device allocation of this chain
+  double *replay = nullptr;
+};
+
+}  // namespace
+
+struct z2_handle {
+  std::string err;
+  int device = 0;
+  int nchains = 0;
+  z2_options opt{};
+  std::vector<ChainHost> ch;
+  ChainDesc *d_desc = nullptr;
+  int *d_order = nullptr;
+  int *d_queue = nullptr;
+  unsigned smem = 0;
+  int grid = 1;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  bool pre_done = false;
+  // unit-op scratch
+  double *u_buf = nullptr;
+  size_t u_n = 0;
+};
+
+static int set_err(z2_handle *h, int code, const char *fmt, ...) {
+  if (h) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    h->err = buf;
+  }
+  return code;
+}
+#define CUDA_TRY(h, x)                                                               \
+  do {                                                                               \
+    cudaError_t e_ = (x);                                                            \
+    if (e_ != cudaSuccess)                                                           \
+      return set_err(h, Z2_ERR_CUDA, "%s failed: %s", #x, cudaGetErrorString(e_));   \
+  } while (0)
+
+// conf_set + conf_transfer for a fresh start (src/fields.f90:311-427, 429-507)
+// with the thermalisation lattice equal to the run lattice.
+static void conf_set_host(const z2_chain_params &p, int N, int Ltrot, std::vector<signed char> &sig,
+                          uint32_t &iq) {
+  const int nb = 2 * N;
+  sig.assign((size_t)nb * Ltrot, 1);
+  iq = fold_seed(p.seed);
+  if (p.absolute == 1) {
+    for (int nt = 0; nt < Ltrot; ++nt)
+      for (int b = 0; b < nb; ++b) sig[(size_t)nt * nb + b] = ranf_host(iq) >= 0.5 ? 1 : -1;
+  } else if (p.absolute == 2) {
+    for (int nt = 0; nt < Ltrot; ++nt)
+      for (int b = 0; b < nb; ++b) {
+        double x1 = ranf_host(iq), x2 = ranf_host(iq);
+        double x = std::sqrt(-2.0 * std::log(x1)) * std::cos(2.0 * M_PI * x2);
+        sig[(size_t)nt * nb + b] = x >= 0.0 ? 1 : -1;
+      }
+  } else if (p.absolute == 3) {
+    // all +1
+  } else if (p.absolute == 4) {
+    for (int nt = 0; nt < Ltrot; ++nt)
+      for (int b = 0; b < nb; ++b) {
+        int s = b / 2, nx = s % p.Nlx + 1, ny = s / p.Nlx + 1;
+        sig[(size_t)nt * nb + b] = ((nx + ny) % 2 == 0) ? 1 : -1;
+      }
+  } else if (p.absolute == 5) {
+    for (int b = 0; b < nb; ++b) {
+      signed char v = ranf_host(iq) >= 0.5 ? 1 : -1;
+      for (int nt = 0; nt < Ltrot; ++nt) sig[(size_t)nt * nb + b] = v;
+    }
+  }
+  // lambda_random_fill: N draws (the lambda field is not on the hot path)
+  for (int i = 0; i < N; ++i) ranf_host(iq);
+}
+
+static size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
+
+static int smem_small_bytes(int N) {
+  size_t off = 0;
+  auto a16 = [](size_t x) { return (x + 15) & ~size_t(15); };
+  off += 8 * Z2_NRED; off += 8 * 8 * N; off += 8 * 2 * N; off += 8 * 2 * N;
+  off += a16(4 * 2 * N); off += a16(4 * 4 * N); off += a16(4 * 4 * N); off += 4 * 16;
+  off += a16(2 * N);
+  return (int)a16(off);
+}
+
+static int default_k(int N) {
+  if (N <= 36) return 32;
+  if (N <= 64) return 32;
+  if (N <= 100) return 16;
+  return 8;
+}
+
+extern "C" int z2_create(z2_handle **out, const z2_chain_params *params, int32_t nchains,
+                         const z2_options *opt) {
+  if (!out || !params || nchains <= 0) return Z2_ERR_ARG;
+  z2_handle *h = new z2_handle();
+  *out = h;
+  h->nchains = nchains;
+  if (opt) h->opt = *opt;
+  h->device = h->opt.device;
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  // ranf multiplier powers
+  {
+    unsigned int pw[33];
+    uint64_t v = 1;
+    for (int i = 0; i <= 32; ++i) { pw[i] = (unsigned)v; v = (v * 48828125ull) & 0x7fffffffull; }
+    CUDA_TRY(h, cudaMemcpyToSymbol(c_ipow, pw, sizeof(pw)));
+  }
+  h->ch.resize(nchains);
+  int smem_needed = 0;
+  for (int c = 0; c < nchains; ++c) {
+    ChainHost &C = h->ch[c];
+    C.p = params[c];
+    const z2_chain_params &p = C.p;
+    if (p.Nlx < 2 || p.Nly < 2 || (p.Nlx % 2) || (p.Nly % 2))
+      return set_err(h, Z2_ERR_ARG, "chain %d: Nlx, Nly must be even and >= 2", c);
+    if (p.Ltrot < 1 || p.Nwrap < 1 || p.Ltrot % p.Nwrap)
+      return set_err(h, Z2_ERR_ARG, "chain %d: Ltrot must be a multiple of Nwrap", c);
+    if (p.absolute < 1 || p.absolute > 5)
+      return set_err(h, Z2_ERR_ARG, "chain %d: incorrect absolute input %d", c, p.absolute);
+    C.N = p.Nlx * p.Nly;
+    if (C.N > 1024) return set_err(h, Z2_ERR_ARG, "chain %d: N = %d exceeds 1024", c, C.N);
+    C.Ltrot = p.Ltrot;
+    C.Nst = p.Ltrot / p.Nwrap;
+    C.nb = 2 * C.N;
+    C.dtau = p.beta / (double)p.Ltrot;
+    C.rt.assign(C.nb, p.RT);
+    if (p.rt_bond) for (int b = 0; b < C.nb; ++b) C.rt[b] = p.rt_bond[b];
+    conf_set_host(p, C.N, C.Ltrot, C.sigma0, C.iseed0);
+    // shared-memory plan
+    const int N = C.N;
+    const int ldg = (N % 2) ? N : N + 1;
+    int small = smem_small_bytes(N);
+    int k = h->opt.delay_k > 0 ? h->opt.delay_k : default_k(N);
+    size_t arena = (size_t)(kSmemMax - small) / 8;
+    size_t nn = (size_t)N * ldg;
+    int g_in = 0;
+    int k2 = 2 * k;
+    if (nn + std::max<size_t>(2 * (size_t)N * k2, kGemmTile) <= arena) g_in = 1;
+    else if (nn + std::max<size_t>(2 * (size_t)N * 4, kGemmTile) <= arena) {
+      g_in = 1;
+      while (k2 > 4 && nn + 2 * (size_t)N * k2 > arena) k2 -= 2;
+    }
+    if (!g_in) {
+      while (k2 > 2 && 2 * (size_t)N * k2 > arena) k2 -= 2;
+    }
+    size_t need = small + 8 * (g_in ? nn + std::max<size_t>(2 * (size_t)N * k2, kGemmTile)
+                                    : std::max<size_t>(2 * (size_t)N * k2, kGemmTile));
+    smem_needed = std::max(smem_needed, (int)need);
+    C.d = ChainDesc{};
+    C.d.N = N; C.d.Lx = p.Nlx; C.d.Ly = p.Nly; C.d.Ltrot = p.Ltrot; C.d.Nwrap = p.Nwrap;
+    C.d.Nst = C.Nst; C.d.nb = C.nb; C.d.half = N / 2; C.d.ldg = ldg; C.d.k2 = k2;
+    C.d.g_in_smem = g_in;
+  }
+  // the launch uses one dynamic smem size; chains planned for a larger
+  // arena still fit because the plan used the maximum.
+  h->smem = (unsigned)std::max(smem_needed, 4096);
+  if ((int)h->smem > kSmemMax) h->smem = kSmemMax;
+  // re-plan with the final arena: G in smem only if it fits h->smem
+  for (auto &C : h->ch) {
+    const int N = C.N;
+    size_t arena = (h->smem - smem_small_bytes(N)) / 8;
+    size_t nn = (size_t)N * C.d.ldg;
+    if (C.d.g_in_smem && nn + std::max<size_t>(2 * (size_t)N * C.d.k2, kGemmTile) > arena)
+      C.d.g_in_smem = 0;
+  }
+  CUDA_TRY(h, cudaFuncSetAttribute(z2_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)h->smem));
+  CUDA_TRY(h, cudaFuncSetAttribute(z2_unit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)h->smem));
+  // device memory and tables
+  for (int c = 0; c < nchains; ++c) {
+    ChainHost &C = h->ch[c];
+    const z2_chain_params &p = C.p;
+    const int N = C.N, nb = C.nb, Lt = C.Ltrot, Nst = C.Nst;
+    HostLattice lat(p.Nlx, p.Nly);
+    if (!lat.ok) return set_err(h, Z2_ERR_ARG, "chain %d: checkerboard groups not of size N/2", c);
+    const size_t NN = (size_t)N * N;
+    std::vector<double> chsh(2 * nb), dlt(2 * nb), stag(N);
+    for (int b = 0; b < nb; ++b) {
+      double alpha = 0.5 * C.dtau * C.rt[b];      // opK_set (src/operator_kin.f90:26)
+      chsh[2 * b] = std::cosh(alpha);
+      chsh[2 * b + 1] = std::sinh(alpha);
+      double a2 = C.dtau * C.rt[b];               // opK_get_delta (src/operator_kin.f90:40-59)
+      double c_new = std::cosh(a2 * 1.0), c_old = std::cosh(a2 * -1.0);
+      double s_new = std::sinh(a2 * 1.0), s_old = std::sinh(a2 * -1.0);
+      dlt[2 * b] = c_new * c_old - s_new * s_old - 1.0;
+      dlt[2 * b + 1] = s_new * c_old - c_new * s_old;
+    }
+    for (int s = 0; s < N; ++s) stag[s] = ((lat.xy[2 * s] + lat.xy[2 * s + 1]) % 2 == 0) ? 1.0 : -1.0;
+    const int W = 2 * p.Nlx - 1, H = 2 * p.Nly - 1;
+    std::vector<double> psh((size_t)W * H);
+    const double PI = std::acos(-1.0);
+    const double qx = PI - 2.0 * PI / (double)p.Nlx;
+    for (int dy = -(p.Nly - 1); dy <= p.Nly - 1; ++dy)
+      for (int dx = -(p.Nlx - 1); dx <= p.Nlx - 1; ++dx)
+        psh[(dx + p.Nlx - 1) + (size_t)(dy + p.Nly - 1) * W] = std::cos(qx * (double)dx + PI * (double)dy);
+    // boson ratio table (src/fields.f90:52-117)
+    double rb[9];
+    {
+      const double alpha = C.dtau * p.J;
+      double gamma = 0.0; bool temporal = false;
+      if (std::fabs(p.h) > kZero) {
+        double ta = std::tanh(C.dtau * p.h);
+        if (ta < 1.0e-300) ta = 1.0e-300;
+        gamma = -0.5 * std::log(ta);
+        temporal = true;
+      }
+      const double lub = std::log(kUpbound);
+      for (int is = 0; is < 3; ++is)
+        for (int it = 0; it < 3; ++it) {
+          double ds = 4.0 * is - 4.0, dt = 4.0 * it - 4.0;
+          double e = alpha * ds;
+          e = std::min(std::max(e, -lub), lub);
+          double r = std::exp(e);
+          if (temporal) {
+            double e2 = gamma * dt;
+            e2 = std::min(std::max(e2, -lub), lub);
+            r = r * std::exp(e2);
+          }
+          rb[is * 3 + it] = r;
+        }
+    }
+    // layout of this chain's device block
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t o = off; off += al256(bytes); return o; };
+    size_t o_bonds = take(4 * lat.bonds.size()), o_groups = take(4 * lat.groups.size());
+    size_t o_bb = take(4 * lat.bbonds.size()), o_plaq = take(4 * lat.plaq.size());
+    size_t o_xy = take(4 * lat.xy.size()), o_nbx = take(4 * lat.nbx.size());
+    size_t o_chsh = take(8 * chsh.size()), o_dlt = take(8 * dlt.size());
+    size_t o_stag = take(8 * stag.size()), o_psh = take(8 * psh.size());
+    size_t o_sigma = take((size_t)nb * Lt);
+    size_t o_mat = take(8 * NN * 10);             // G, UR, VR, ULT, VL, W0..W4
+    size_t o_vec = take(8 * (size_t)N * 2);       // DR, DL
+    size_t o_stk = take(8 * NN * 4 * (Nst + 1));  // URs, VRs, ULTs, VLs
+    size_t o_stv = take(8 * (size_t)N * 2 * (Nst + 1));
+    size_t o_tau = take(8 * NN * 8);              // G00, Gtt, Gt0, G0t, URd, VRd, ULTd, VLd
+    size_t o_tauv = take(8 * (size_t)N * 2);      // DRd, DLd
+    size_t o_big = take(8 * NN * 16);             // B0..B3 (2N x 2N)
+    size_t o_otau = take(8 * (size_t)7 * Lt * N);
+    size_t o_grad = take(8 * (size_t)nb);
+    size_t o_acc = take(8 * A_COUNT);
+    size_t o_misc = take(64);                     // rng, replay_pos, status
+    size_t o_dec = 0, o_rat = 0;
+    if (h->opt.record) { o_dec = take((size_t)2 * Lt * nb); o_rat = take(8 * (size_t)2 * Lt * nb); }
+    C.bytes = off;
+    char *base = nullptr;
+    if (cudaMalloc(&base, C.bytes) != cudaSuccess)
+      return set_err(h, Z2_ERR_NOMEM, "chain %d: cudaMalloc of %zu bytes failed", c, C.bytes);
+    C.base = base;
+    CUDA_TRY(h, cudaMemset(base, 0, C.bytes));
+    auto up = [&](size_t o, const void *src, size_t bytes) {
+      return cudaMemcpy(base + o, src, bytes, cudaMemcpyHostToDevice);
+    };
+    CUDA_TRY(h, up(o_bonds, lat.bonds.data(), 4 * lat.bonds.size()));
+    CUDA_TRY(h, up(o_groups, lat.groups.data(), 4 * lat.groups.size()));
+    CUDA_TRY(h, up(o_bb, lat.bbonds.data(), 4 * lat.bbonds.size()));
+    CUDA_TRY(h, up(o_plaq, lat.plaq.data(), 4 * lat.plaq.size()));
+    CUDA_TRY(h, up(o_xy, lat.xy.data(), 4 * lat.xy.size()));
+    CUDA_TRY(h, up(o_nbx, lat.nbx.data(), 4 * lat.nbx.size()));
+    CUDA_TRY(h, up(o_chsh, chsh.data(), 8 * chsh.size()));
+    CUDA_TRY(h, up(o_dlt, dlt.data(), 8 * dlt.size()));
+    CUDA_TRY(h, up(o_stag, stag.data(), 8 * stag.size()));
+    CUDA_TRY(h, up(o_psh, psh.data(), 8 * psh.size()));
+    CUDA_TRY(h, up(o_sigma, C.sigma0.data(), C.sigma0.size()));
+    ChainDesc &d = C.d;
+    d.beta = p.beta; d.dtau = C.dtau;
+    d.eP = std::exp(C.dtau * p.mu); d.eM = std::exp(-C.dtau * p.mu);
+    d.rt_scalar = p.RT;
+    for (int q = 0; q < 9; ++q) d.rb[q] = rb[q];
+    d.use_kin = p.RT > kZero ? 1 : 0;
+    d.hzero = std::fabs(p.h) <= kZero ? 1 : 0;
+    d.bonds = (const int *)(base + o_bonds); d.groups = (const int *)(base + o_groups);
+    d.bbonds = (const int *)(base + o_bb); d.plaq = (const int *)(base + o_plaq);
+    d.xy = (const int *)(base + o_xy); d.nbx = (const int *)(base + o_nbx);
+    d.chsh = (const double *)(base + o_chsh); d.dlt = (const double *)(base + o_dlt);
+    d.stag = (const double *)(base + o_stag); d.pshift = (const double *)(base + o_psh);
+    d.sigma = (signed char *)(base + o_sigma);
+    double *m = (double *)(base + o_mat);
+    d.G = m; d.UR = m + NN; d.VR = m + 2 * NN; d.ULT = m + 3 * NN; d.VL = m + 4 * NN;
+    d.W0 = m + 5 * NN; d.W1 = m + 6 * NN; d.W2 = m + 7 * NN; d.W3 = m + 8 * NN; d.W4 = m + 9 * NN;
+    double *v = (double *)(base + o_vec);
+    d.DR = v; d.DL = v + N;
+    double *st = (double *)(base + o_stk);
+    d.URs = st; d.VRs = st + NN * (Nst + 1); d.ULTs = st + 2 * NN * (Nst + 1); d.VLs = st + 3 * NN * (Nst + 1);
+    double *sv = (double *)(base + o_stv);
+    d.DRs = sv; d.DLs = sv + (size_t)N * (Nst + 1);
+    double *tm = (double *)(base + o_tau);
+    d.G00 = tm; d.Gtt = tm + NN; d.Gt0 = tm + 2 * NN; d.G0t = tm + 3 * NN;
+    d.URd = tm + 4 * NN; d.VRd = tm + 5 * NN; d.ULTd = tm + 6 * NN; d.VLd = tm + 7 * NN;
+    double *tv = (double *)(base + o_tauv);
+    d.DRd = tv; d.DLd = tv + N;
+    double *bg = (double *)(base + o_big);
+    d.B0 = bg; d.B1 = bg + 4 * NN; d.B2 = bg + 8 * NN; d.B3 = bg + 12 * NN;
+    d.obs_tau = (double *)(base + o_otau);
+    d.grad = (double *)(base + o_grad);
+    d.acc = (double *)(base + o_acc);
+    char *misc = base + o_misc;
+    d.rng = (unsigned int *)misc;
+    d.replay_pos = (long long *)(misc + 8);
+    d.status = (int *)(misc + 16);
+    d.replay = nullptr; d.nreplay = 0;
+    d.dec = h->opt.record ? (unsigned char *)(base + o_dec) : nullptr;
+    d.ratios = h->opt.record ? (double *)(base + o_rat) : nullptr;
+    uint32_t s0 = C.iseed0;
+    CUDA_TRY(h, cudaMemcpy(d.rng, &s0, 4, cudaMemcpyHostToDevice));
+  }
+  // descriptors, LPT order
+  CUDA_TRY(h, cudaMalloc(&h->d_desc, sizeof(ChainDesc) * nchains));
+  CUDA_TRY(h, cudaMalloc(&h->d_order, sizeof(int) * nchains));
+  CUDA_TRY(h, cudaMalloc(&h->d_queue, sizeof(int)));
+  {
+    std::vector<ChainDesc> dd(nchains);
+    for (int c = 0; c < nchains; ++c) dd[c] = h->ch[c].d;
+    CUDA_TRY(h, cudaMemcpy(h->d_desc, dd.data(), sizeof(ChainDesc) * nchains, cudaMemcpyHostToDevice));
+    std::vector<int> order(nchains);
+    for (int c = 0; c < nchains; ++c) order[c] = c;
+    auto cost = [&](int c) {
+      const ChainHost &C = h->ch[c];
+      double n = C.N;
+      return (double)C.Ltrot * n * n * (n / C.p.Nwrap * 14.0 + 80.0);
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost(a) > cost(b); });
+    CUDA_TRY(h, cudaMemcpy(h->d_order, order.data(), sizeof(int) * nchains, cudaMemcpyHostToDevice));
+  }
+  int nsm = 0, occ = 0;
+  CUDA_TRY(h, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
+  CUDA_TRY(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, z2_chain_kernel, Z2_NT, h->smem));
+  if (occ < 1) occ = 1;
+  h->grid = std::min(nchains, nsm * occ);
+  CUDA_TRY(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  CUDA_TRY(h, cudaEventCreate(&h->ev0));
+  CUDA_TRY(h, cudaEventCreate(&h->ev1));
+  return Z2_OK;
+}
+
+extern "C" int z2_destroy(z2_handle *h) {
+  if (!h) return Z2_OK;
+  cudaSetDevice(h->device);
+  for (auto &C : h->ch) {
+    if (C.base) cudaFree(C.base);
+    if (C.replay) cudaFree(C.replay);
+  }
+  if (h->d_desc) cudaFree(h->d_desc);
+  if (h->d_order) cudaFree(h->d_order);
+  if (h->d_queue) cudaFree(h->d_queue);
+  if (h->u_buf) cudaFree(h->u_buf);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return Z2_OK;
+}
+
+extern "C" const char *z2_last_error(const z2_handle *h) { return h ? h->err.c_str() : "null handle"; }
+
+static int check_chain(const z2_handle *h, int chain) {
+  if (!h) return Z2_ERR_ARG;
+  if (chain < 0 || chain >= h->nchains)
+    return set_err(const_cast<z2_handle *>(h), Z2_ERR_ARG, "chain %d out of range", chain);
+  return Z2_OK;
+}
+
+extern "C" int z2_chain_dims(const z2_handle *h, int32_t chain, int32_t *N, int32_t *Ltrot,
+                             int32_t *Nst) {
+  int r = check_chain(h, chain);
+  if (r) return r;
+  const ChainHost &C = h->ch[chain];
+  if (N) *N = C.N;
+  if (Ltrot) *Ltrot = C.Ltrot;
+  if (Nst) *Nst = C.Nst;
+  return Z2_OK;
+}
+
+extern "C" int z2_set_config(z2_handle *h, int32_t chain, const double *sigma, int32_t iseed) {
+  int r = check_chain(h, chain);
+  if (r) return r;
+  ChainHost &C = h->ch[chain];
+  std::vector<signed char> s((size_t)C.nb * C.Ltrot);
+  for (size_t i = 0; i < s.size(); ++i) {
+    if (sigma[i] != 1.0 && sigma[i] != -1.0)
+      return set_err(h, Z2_ERR_ARG, "sigma[%zu] = %g is not +-1", i, sigma[i]);
+    s[i] = sigma[i] > 0 ? 1 : -1;
+  }
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  CUDA_TRY(h, cudaMemcpy(C.d.sigma, s.data(), s.size(), cudaMemcpyHostToDevice));
+  uint32_t st = (uint32_t)iseed;
+  CUDA_TRY(h, cudaMemcpy(C.d.rng, &st, 4, cudaMemcpyHostToDevice));
+  h->pre_done = false;
+  return Z2_OK;
+}
+
+extern "C" int z2_get_config(const z2_handle *h, int32_t chain, double *sigma, int32_t *iseed) {
+  int r = check_chain(h, chain);
+  if (r) return r;
+  z2_handle *hh = const_cast<z2_handle *>(h);
+  const ChainHost &C = h->ch[chain];
+  std::vector<signed char> s((size_t)C.nb * C.Ltrot);
+  CUDA_TRY(hh, cudaSetDevice(h->device));
+  CUDA_TRY(hh, cudaMemcpy(s.data(), C.d.sigma, s.size(), cudaMemcpyDeviceToHost));
+  if (sigma) for (size_t i = 0; i < s.size(); ++i) sigma[i] = (double)s[i];
+  if (iseed) {
+    uint32_t st;
+    CUDA_TRY(hh, cudaMemcpy(&st, C.d.rng, 4, cudaMemcpyDeviceToHost));
+    *iseed = (int32_t)st;
+  }
+  return Z2_OK;
+}
+
+static int launch_chains(z2_handle *h, int op, int nsweep, int toggle, float *ms) {
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  CUDA_TRY(h, cudaMemsetAsync(h->d_queue, 0, sizeof(int), h->stream));
+  if (ms) CUDA_TRY(h, cudaEventRecord(h->ev0, h->stream));
+  z2_chain_kernel<<<h->grid, Z2_NT, h->smem, h->stream>>>(h->d_desc, h->d_order, h->nchains,
+                                                          h->d_queue, op, nsweep, toggle, h->smem);
+  CUDA_TRY(h, cudaGetLastError());
+  if (ms) CUDA_TRY(h, cudaEventRecord(h->ev1, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  if (ms) CUDA_TRY(h, cudaEventElapsedTime(ms, h->ev0, h->ev1));
+  // status flags
+  for (int c = 0; c < h->nchains; ++c) {
+    int st = 0;
+    CUDA_TRY(h, cudaMemcpy(&st, h->ch[c].d.status, 4, cudaMemcpyDeviceToHost));
+    if (st & ST_NONFINITE)
+      return set_err(h, Z2_ERR_NONFINITE, "chain %d: non-finite Green's function", c);
+  }
+  return Z2_OK;
+}
+
+extern "C" int z2_pre(z2_handle *h) {
+  if (!h) return Z2_ERR_ARG;
+  int r = launch_chains(h, OP_PRE, 0, 0, nullptr);
+  if (r == Z2_OK) h->pre_done = true;
+  return r;
+}
+
+extern "C" int z2_sweep_timed(z2_handle *h, int32_t nsweep, int32_t toggle, float *ms) {
+  if (!h) return Z2_ERR_ARG;
+  if (!h->pre_done) return set_err(h, Z2_ERR_STATE, "z2_pre must run before z2_sweep");
+  if (nsweep < 1) return set_err(h, Z2_ERR_ARG, "nsweep must be >= 1");
+  return launch_chains(h, OP_SWEEP, nsweep, toggle, ms);
+}
+
+extern "C" int z2_sweep(z2_handle *h, int32_t nsweep, int32_t toggle) {
+  return z2_sweep_timed(h, nsweep, toggle, nullptr);
+}
+
+extern "C" int z2_get_green(const z2_handle *h, int32_t chain, double *G) {
+  int r = check_chain(h, chain);
+  if (r) return r;
+  z2_handle *hh = const_cast<z2_handle *>(h);
+  const ChainHost &C = h->ch[chain];
+  CUDA_TRY(hh, cudaSetDevice(h->device));
+  CUDA_TRY(hh, cudaMemcpy(G, C.d.G, sizeof(double) * C.N * C.N, cudaMemcpyDeviceToHost));
+  return Z2_OK;
+}
+
+extern "C" int z2_get_obs_equal(const z2_handle *h, int32_t chain, double out[Z2_NOBS_EQ]) {
+  int r = check_chain(h, chain);
+  if (r) return r;
+  z2_handle *hh = const_cast<z2_handle *>(h);
+  CUDA_TRY(hh, cudaSetDevice(h->device));
+  CUDA_TRY(hh, cudaMemcpy(out, h->ch[chain].d.acc + A_BIN0, sizeof(double) * Z2_NOBS_EQ,
+                          cudaMemcpyDeviceToHost));
+  return Z2_OK;
+}
+
+extern "C" int z2_get_obs_tau(const z2_handle *h, int32_t chain, double *out) {
+  int r = check_chain(h, chain);
+  if (r) return r;
+  z2_handle *hh = const_cast<z2_handle *>(h);
+  const ChainHost &C = h->ch[chain];
+  CUDA_TRY(hh, cudaSetDevice(h->device));
+  CUDA_TRY(hh, cudaMemcpy(out, C.d.obs_tau, sizeof(double) * 7 * C.Ltrot * C.N,
+                          cudaMemcpyDeviceToHost));
+  return Z2_OK;
+}
+
+extern "C" int z2_get_stats(const z2_handle *h, int32_t chain, double out[Z2_NSTATS]) {
+  int r = check_chain(h, chain);
+  if (r) return r;
+  z2_handle *hh = const_cast<z2_handle *>(h);
+  double a[A_COUNT];
+  CUDA_TRY(hh, cudaSetDevice(h->device));
+  CUDA_TRY(hh, cudaMemcpy(a, h->ch[chain].d.acc, sizeof(a), cudaMemcpyDeviceToHost));
+  out[0] = a[A_ACC]; out[1] = a[A_XMAX]; out[2] = a[A_XMEAN];
+  out[3] = a[A_TXMAX0]; out[4] = a[A_TXMAX1]; out[5] = a[A_TXMAX2];
+  out[6] = a[A_TXMEAN0]; out[7] = a[A_TXMEAN1]; out[8] = a[A_TXMEAN2];
+  out[9] = a[A_ACC_NUM]; out[10] = a[A_ACC_DEN]; out[11] = a[A_DRAWS];
+  out[12] = a[A_NOBS]; out[13] = a[A_NOBST];
+  return Z2_OK;
+}
+
+static int upload_desc(z2_handle *h, int chain) {
+  CUDA_TRY(h, cudaMemcpy(h->d_desc + chain, &h->ch[chain].d, sizeof(ChainDesc),
+                         cudaMemcpyHostToDevice));
+  return Z2_OK;
+}
+
+extern "C" int z2_set_replay(z2_handle *h, int32_t chain, const double *rr, size_t n) {
+  int r = check_chain(h, chain);
+  if (r) return r;
+  ChainHost &C = h->ch[chain];
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  if (C.replay) { cudaFree(C.replay); C.replay = nullptr; }
+  C.d.replay = nullptr; C.d.nreplay = 0;
+  if (n > 0) {
+    CUDA_TRY(h, cudaMalloc(&C.replay, n * sizeof(double)));
+    CUDA_TRY(h, cudaMemcpy(C.replay, rr, n * sizeof(double), cudaMemcpyHostToDevice));
+    C.d.replay = C.replay; C.d.nreplay = (long long)n;
+  }
+  long long z = 0;
+  CUDA_TRY(h, cudaMemcpy(C.d.replay_pos, &z, sizeof(z), cudaMemcpyHostToDevice));
+  return upload_desc(h, chain);
+}
+
+extern "C" int z2_get_decisions(const z2_handle *h, int32_t chain, uint8_t *dec, double *ratios,
+                                size_t n) {
+  int r = check_chain(h, chain);
+  if (r) return r;
+  z2_handle *hh = const_cast<z2_handle *>(h);
+  const ChainHost &C = h->ch[chain];
+  if (!C.d.dec) return set_err(hh, Z2_ERR_STATE, "decisions are recorded only with options.record = 1");
+  size_t tot = (size_t)2 * C.Ltrot * C.nb;
+  if (n > tot) n = tot;
+  CUDA_TRY(hh, cudaSetDevice(h->device));
+  if (dec) CUDA_TRY(hh, cudaMemcpy(dec, C.d.dec, n, cudaMemcpyDeviceToHost));
+  if (ratios) CUDA_TRY(hh, cudaMemcpy(ratios, C.d.ratios, n * sizeof(double), cudaMemcpyDeviceToHost));
+  return Z2_OK;
+}
+
+extern "C" int z2_logdet_grad(z2_handle *h, int32_t chain, double *logdet, double *dlogdet_dt,
+                              double *dlogdet_dmu) {
+  int r = check_chain(h, chain);
+  if (r) return r;
+  ChainHost &C = h->ch[chain];
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  // run only this chain: a one-entry order list pointing at it
+  int *d_one = nullptr;
+  CUDA_TRY(h, cudaMalloc(&d_one, sizeof(int)));
+  CUDA_TRY(h, cudaMemcpy(d_one, &chain, sizeof(int), cudaMemcpyHostToDevice));
+  CUDA_TRY(h, cudaMemsetAsync(h->d_queue, 0, sizeof(int), h->stream));
+  z2_chain_kernel<<<1, Z2_NT, h->smem, h->stream>>>(h->d_desc, d_one, 1, h->d_queue, OP_LOGDET, 0,
+                                                     0, h->smem);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(d_one);
+  if (e != cudaSuccess) return set_err(h, Z2_ERR_CUDA, "logdet kernel: %s", cudaGetErrorString(e));
+  double a[A_COUNT];
+  CUDA_TRY(h, cudaMemcpy(a, C.d.acc, sizeof(a), cudaMemcpyDeviceToHost));
+  if (logdet) *logdet = a[A_LOGDET];
+  if (dlogdet_dmu) *dlogdet_dmu = a[A_DMU];
+  if (dlogdet_dt) CUDA_TRY(h, cudaMemcpy(dlogdet_dt, C.d.grad, sizeof(double) * C.nb, cudaMemcpyDeviceToHost));
+  h->pre_done = true;
+  return Z2_OK;
+}
+
+// ---- module-level mirrors ----
+static int unit_scratch(z2_handle *h, size_t doubles) {
+  if (h->u_n >= doubles) return Z2_OK;
+  if (h->u_buf) cudaFree(h->u_buf);
+  h->u_buf = nullptr; h->u_n = 0;
+  CUDA_TRY(h, cudaMalloc(&h->u_buf, doubles * sizeof(double)));
+  h->u_n = doubles;
+  return Z2_OK;
+}
+
+static int run_unit(z2_handle *h, int chain, int op, const UnitArgs &a) {
+  z2_unit_kernel<<<1, Z2_NT, h->smem, h->stream>>>(h->d_desc + chain, op, a, h->smem);
+  CUDA_TRY(h, cudaGetLastError());
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return Z2_OK;
+}
+
+static int mmult(z2_handle *h, int chain, double *M, int nt, int nflag, int op) {
+  int r = check_chain(h, chain);
+  if (r) return r;
+  ChainHost &C = h->ch[chain];
+  if (nt < 1 || nt > C.Ltrot) return set_err(h, Z2_ERR_ARG, "nt = %d out of 1..Ltrot", nt);
+  if (nflag != 1 && nflag != -1) return set_err(h, Z2_ERR_ARG, "incorrect nflag %d", nflag);
+  const size_t NN = (size_t)C.N * C.N;
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  if ((r = unit_scratch(h, NN))) return r;
+  CUDA_TRY(h, cudaMemcpy(h->u_buf, M, NN * 8, cudaMemcpyHostToDevice));
+  UnitArgs a{};
+  a.M = h->u_buf; a.nt = nt; a.nflag = nflag;
+  if ((r = run_unit(h, chain, op, a))) return r;
+  CUDA_TRY(h, cudaMemcpy(M, h->u_buf, NN * 8, cudaMemcpyDeviceToHost));
+  return Z2_OK;
+}
+
+extern "C" int z2_opk_mmult_R(z2_handle *h, int32_t chain, double *M, int32_t nt, int32_t nflag) {
+  return mmult(h, chain, M, nt, nflag, U_MMULT_R);
+}
+extern "C" int z2_opk_mmult_L(z2_handle *h, int32_t chain, double *M, int32_t nt, int32_t nflag) {
+  return mmult(h, chain, M, nt, nflag, U_MMULT_L);
+}
+
+static void transpose_host(const double *src, double *dst, int N) {
+  for (int j = 0; j < N; ++j)
+    for (int i = 0; i < N; ++i) dst[j + (size_t)i * N] = src[i + (size_t)j * N];
+}
+
+static int stab_u(z2_handle *h, int chain, double *U, double *D, double *V, bool left) {
+  int r = check_chain(h, chain);
+  if (r) return r;
+  ChainHost &C = h->ch[chain];
+  const int N = C.N;
+  const size_t NN = (size_t)N * N;
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  if ((r = unit_scratch(h, 2 * NN + N))) return r;
+  std::vector<double> tmp(NN);
+  const double *Usrc = U;
+  if (left) { transpose_host(U, tmp.data(), N); Usrc = tmp.data(); }
+  CUDA_TRY(h, cudaMemcpy(h->u_buf, Usrc, NN * 8, cudaMemcpyHostToDevice));
+  CUDA_TRY(h, cudaMemcpy(h->u_buf + NN, V, NN * 8, cudaMemcpyHostToDevice));
+  CUDA_TRY(h, cudaMemcpy(h->u_buf + 2 * NN, D, N * 8, cudaMemcpyHostToDevice));
+  UnitArgs a{};
+  a.U = h->u_buf; a.V = h->u_buf + NN; a.D = h->u_buf + 2 * NN;
+  if ((r = run_unit(h, chain, left ? U_STAB_UL : U_STAB_UR, a))) return r;
+  CUDA_TRY(h, cudaMemcpy(tmp.data(), h->u_buf, NN * 8, cudaMemcpyDeviceToHost));
+  if (left) transpose_host(tmp.data(), U, N);
+  else memcpy(U, tmp.data(), NN * 8);
+  CUDA_TRY(h, cudaMemcpy(V, h->u_buf + NN, NN * 8, cudaMemcpyDeviceToHost));
+  CUDA_TRY(h, cudaMemcpy(D, h->u_buf + 2 * NN, N * 8, cudaMemcpyDeviceToHost));
+  return Z2_OK;
+}
+
+extern "C" int z2_stab_UR(z2_handle *h, int32_t chain, double *U, double *D, double *V) {
+  return stab_u(h, chain, U, D, V, false);
+}
+extern "C" int z2_stab_UL(z2_handle *h, int32_t chain, double *U, double *D, double *V) {
+  return stab_u(h, chain, U, D, V, true);
+}
+
+static int upload_udv(z2_handle *h, int N, const double *UR, const double *DR, const double *VR,
+                      const double *UL, const double *DL, const double *VL, size_t extra,
+                      UnitArgs &a) {
+  const size_t NN = (size_t)N * N;
+  int r = unit_scratch(h, 4 * NN + 2 * N + extra);
+  if (r) return r;
+  std::vector<double> ult(NN);
+  transpose_host(UL, ult.data(), N);
+  double *b = h->u_buf;
+  CUDA_TRY(h, cudaMemcpy(b, UR, NN * 8, cudaMemcpyHostToDevice));
+  CUDA_TRY(h, cudaMemcpy(b + NN, VR, NN * 8, cudaMemcpyHostToDevice));
+  CUDA_TRY(h, cudaMemcpy(b + 2 * NN, ult.data(), NN * 8, cudaMemcpyHostToDevice));
+  CUDA_TRY(h, cudaMemcpy(b + 3 * NN, VL, NN * 8, cudaMemcpyHostToDevice));
+  CUDA_TRY(h, cudaMemcpy(b + 4 * NN, DR, N * 8, cudaMemcpyHostToDevice));
+  CUDA_TRY(h, cudaMemcpy(b + 4 * NN + N, DL, N * 8, cudaMemcpyHostToDevice));
+  a.UR = b; a.VR = b + NN; a.ULT = b + 2 * NN; a.VL = b + 3 * NN;
+  a.DR = b + 4 * NN; a.DL = b + 4 * NN + N;
+  return Z2_OK;
+}
+
+extern "C" int z2_stab_green(z2_handle *h, int32_t chain, const double *UR, const double *DR,
+                             const double *VR, const double *UL, const double *DL,
+                             const double *VL, int32_t nt, double *G) {
+  int r = check_chain(h, chain);
+  if (r) return r;
+  ChainHost &C = h->ch[chain];
+  const int N = C.N;
+  const size_t NN = (size_t)N * N;
+  if (nt < 0 || nt > C.Ltrot) return set_err(h, Z2_ERR_ARG, "illegal nt = %d in stab_green", nt);
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  UnitArgs a{};
+  if ((r = upload_udv(h, N, UR, DR, VR, UL, DL, VL, NN, a))) return r;
+  a.G = h->u_buf + 4 * NN + 2 * N;
+  a.nt = nt;
+  if ((r = run_unit(h, chain, U_STAB_GREEN, a))) return r;
+  CUDA_TRY(h, cudaMemcpy(G, a.G, NN * 8, cudaMemcpyDeviceToHost));
+  return Z2_OK;
+}
+
+extern "C" int z2_stab_green_big(z2_handle *h, int32_t chain, const double *UR, const double *DR,
+                                 const double *VR, const double *UL, const double *DL,
+                                 const double *VL, double *G00, double *G0t, double *Gt0,
+                                 double *Gtt) {
+  int r = check_chain(h, chain);
+  if (r) return r;
+  ChainHost &C = h->ch[chain];
+  const int N = C.N;
+  const size_t NN = (size_t)N * N;
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  UnitArgs a{};
+  if ((r = upload_udv(h, N, UR, DR, VR, UL, DL, VL, 4 * NN, a))) return r;
+  double *o = h->u_buf + 4 * NN + 2 * N;
+  a.G = o; a.G0t = o + NN; a.Gt0 = o + 2 * NN; a.Gtt = o + 3 * NN;
+  if ((r = run_unit(h, chain, U_STAB_GREEN_BIG, a))) return r;
+  CUDA_TRY(h, cudaMemcpy(G00, a.G, NN * 8, cudaMemcpyDeviceToHost));
+  CUDA_TRY(h, cudaMemcpy(G0t, a.G0t, NN * 8, cudaMemcpyDeviceToHost));
+  CUDA_TRY(h, cudaMemcpy(Gt0, a.Gt0, NN * 8, cudaMemcpyDeviceToHost));
+  CUDA_TRY(h, cudaMemcpy(Gtt, a.Gtt, NN * 8, cudaMemcpyDeviceToHost));
+  return Z2_OK;
+}

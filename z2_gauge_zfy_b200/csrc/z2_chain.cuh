@@ -1,0 +1,760 @@
+// z2_chain.cuh -- per-chain DQMC drivers run by one CTA.
+//
+// Restates the reference's hot path (src/local_sweep.f90, src/localK.f90,
+// src/multiply.f90, src/operator_kin.f90, src/stabilization.f90,
+// src/dynamics.f90, src/obser_equal.f90, src/obser_tau.f90) for one spin
+// sector in real FP64.  Orders of operations follow the reference; the
+// implementation is B200-first: G stays in shared memory across a slice,
+// accepted flips are queued as rank-2 factors and flushed as one rank-2k
+// update, and the U factors of the UDV chains are propagated lazily (all
+// Nwrap slices at once, right before the stabilization that needs them).
+#pragma once
+#include "z2_linalg.cuh"
+
+// Checkerboard group order of one B (src/operator_kin.f90:74-85).
+__device__ __constant__ int c_gorder[8] = {0, 1, 2, 3, 3, 2, 1, 0};
+
+// ---------------------------------------------------------------------------
+// Shared-memory layout
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+
+__device__ Smem make_smem(const ChainDesc &c, unsigned char *base, size_t smem_bytes) {
+  Smem s;
+  const int N = c.N;
+  size_t off = 0;
+  s.red = (double *)(base + off); off += sizeof(double) * Z2_NRED;
+  s.vec = (double *)(base + off); off += sizeof(double) * 8 * N;
+  s.tc = (double *)(base + off); off += sizeof(double) * 2 * N;
+  s.ts = (double *)(base + off); off += sizeof(double) * 2 * N;
+  s.ivec = (int *)(base + off); off += align16(sizeof(int) * 2 * N);
+  s.tp = (int *)(base + off); off += align16(sizeof(int) * 4 * N);
+  s.bond = (int *)(base + off); off += align16(sizeof(int) * 4 * N);
+  s.flag = (int *)(base + off); off += sizeof(int) * 16;
+  s.sig = (signed char *)(base + off); off += align16(2 * N);
+  off = align16(off);
+  s.arena = (double *)(base + off);
+  const size_t arena_doubles = (smem_bytes - off) / sizeof(double);
+  const size_t nn = (size_t)N * c.ldg;
+  if (c.g_in_smem) {
+    s.G = s.arena; s.ldg = c.ldg;
+    s.X = s.arena + nn; s.Yt = s.X + (size_t)N * c.k2;
+    s.Wq = s.arena; s.ldq = c.ldg;
+    s.tile = s.arena + nn;
+    s.tile_doubles = (int)(arena_doubles - nn);
+  } else {
+    s.G = c.G; s.ldg = N;
+    s.X = s.arena; s.Yt = s.X + (size_t)N * c.k2;
+    s.Wq = c.W4;
+    s.ldq = N;
+    s.tile = s.arena;
+    s.tile_doubles = (int)arena_doubles;
+  }
+  return s;
+}
+
+// ---------------------------------------------------------------------------
+// Checkerboard kinetic propagator (src/operator_kin.f90:61-179)
+// ---------------------------------------------------------------------------
+// Slice table in group order: position q = g*half + k holds bond groups[q].
+__device__ __noinline__ void build_table(const ChainDesc &c, const Smem &s, int nt) {
+  const signed char *sg = c.sigma + (size_t)(nt - 1) * c.nb;
+  for (int q = threadIdx.x; q < c.nb; q += Z2_NT) {
+    int b = c.groups[q];
+    s.tp[2 * q] = c.bonds[2 * b];
+    s.tp[2 * q + 1] = c.bonds[2 * b + 1];
+    s.tc[q] = c.chsh[2 * b];
+    s.ts[q] = (double)sg[b] * c.chsh[2 * b + 1];   // sinh(alpha*sigma) = sigma*sinh(alpha)
+  }
+  __syncthreads();
+}
+
+// M <- B^nflag M : rows P1, P2 rotated by [[C,S],[S,C]] (process_group).
+__device__ __noinline__ void kin_rows(const ChainDesc &c, const Smem &s, double *M, int ld, int ncols,
+                         int nflag) {
+  const int half = c.half;
+  const int work = half * ncols;
+  const double fl = (double)nflag;
+  for (int p = 0; p < 8; ++p) {
+    const int g0 = c_gorder[p] * half;
+    for (int idx = threadIdx.x; idx < work; idx += Z2_NT) {
+      int kq = idx / ncols;
+      int col = idx - kq * ncols;
+      int q = g0 + kq;
+      int p1 = s.tp[2 * q], p2 = s.tp[2 * q + 1];
+      double C = s.tc[q], S = fl * s.ts[q];
+      double *mc = M + (size_t)col * ld;
+      double a = mc[p1], b = mc[p2];
+      mc[p1] = C * a + S * b;
+      mc[p2] = S * a + C * b;
+    }
+    __syncthreads();
+  }
+}
+
+// M <- M B^nflag : columns P1, P2 rotated (process_group_L).
+__device__ __noinline__ void kin_cols(const ChainDesc &c, const Smem &s, double *M, int ld, int nrows,
+                         int nflag) {
+  const int half = c.half;
+  const int work = half * nrows;
+  const double fl = (double)nflag;
+  for (int p = 0; p < 8; ++p) {
+    const int g0 = c_gorder[p] * half;
+    for (int idx = threadIdx.x; idx < work; idx += Z2_NT) {
+      int kq = idx / nrows;
+      int row = idx - kq * nrows;
+      int q = g0 + kq;
+      int p1 = s.tp[2 * q], p2 = s.tp[2 * q + 1];
+      double C = s.tc[q], S = fl * s.ts[q];
+      double a = M[row + (size_t)p1 * ld], b = M[row + (size_t)p2 * ld];
+      M[row + (size_t)p1 * ld] = a * C + b * S;
+      M[row + (size_t)p2 * ld] = a * S + b * C;
+    }
+    __syncthreads();
+  }
+}
+
+// One group (one factor E_g) of B applied to rows / columns.
+__device__ __noinline__ void kin_group_rows(const ChainDesc &c, const Smem &s, double *M, int ld, int ncols,
+                               int g, int nflag) {
+  const int half = c.half, work = half * ncols, g0 = g * half;
+  const double fl = (double)nflag;
+  for (int idx = threadIdx.x; idx < work; idx += Z2_NT) {
+    int kq = idx / ncols, col = idx - kq * ncols, q = g0 + kq;
+    int p1 = s.tp[2 * q], p2 = s.tp[2 * q + 1];
+    double C = s.tc[q], S = fl * s.ts[q];
+    double *mc = M + (size_t)col * ld;
+    double a = mc[p1], b = mc[p2];
+    mc[p1] = C * a + S * b;
+    mc[p2] = S * a + C * b;
+  }
+  __syncthreads();
+}
+__device__ __noinline__ void kin_group_cols(const ChainDesc &c, const Smem &s, double *M, int ld, int nrows,
+                               int g, int nflag) {
+  const int half = c.half, work = half * nrows, g0 = g * half;
+  const double fl = (double)nflag;
+  for (int idx = threadIdx.x; idx < work; idx += Z2_NT) {
+    int kq = idx / nrows, row = idx - kq * nrows, q = g0 + kq;
+    int p1 = s.tp[2 * q], p2 = s.tp[2 * q + 1];
+    double C = s.tc[q], S = fl * s.ts[q];
+    double a = M[row + (size_t)p1 * ld], b = M[row + (size_t)p2 * ld];
+    M[row + (size_t)p1 * ld] = a * C + b * S;
+    M[row + (size_t)p2 * ld] = a * S + b * C;
+  }
+  __syncthreads();
+}
+
+// Apply B-multiplications to a global N x N matrix, staging it through the
+// arena when it fits (the arena must be free).
+__device__ __noinline__ void kin_global(const ChainDesc &c, const Smem &s, double *M, int row_flag,
+                           int col_flag) {
+  const int N = c.N;
+  if (c.g_in_smem) {
+    double *A = s.arena;
+    blk_copy(A, c.ldg, M, N, N, N);
+    if (row_flag) kin_rows(c, s, A, c.ldg, N, row_flag);
+    if (col_flag) kin_cols(c, s, A, c.ldg, N, col_flag);
+    blk_copy(M, N, A, c.ldg, N, N);
+  } else {
+    if (row_flag) kin_rows(c, s, M, N, N, row_flag);
+    if (col_flag) kin_cols(c, s, M, N, N, col_flag);
+  }
+}
+
+// Lazily propagated U factors.  R chain: for nt' = lo..hi, U <- B_nt' U then
+// U *= e^{dtau mu} (LocalK_prop_R + propT_R, src/localK.f90:395-396,
+// src/multiply.f90:106).  L chain (ULT = UL^T, B symmetric): for nt' = hi
+// down to lo, ULT *= e^{dtau mu} then ULT <- B_nt' ULT (propT_L + prop_L,
+// src/multiply.f90:91, src/localK.f90:370).
+__device__ __noinline__ void apply_pending_R(const ChainDesc &c, const Smem &s, double *A, int lda, int lo,
+                                int hi, bool kin) {
+  for (int t = lo; t <= hi; ++t) {
+    if (kin) {
+      build_table(c, s, t);
+      kin_rows(c, s, A, lda, c.N, 1);
+    }
+    if (c.eP != 1.0) blk_scale(A, lda, c.N, c.N, c.eP);
+  }
+}
+__device__ __noinline__ void apply_pending_L(const ChainDesc &c, const Smem &s, double *A, int lda, int lo,
+                                int hi) {
+  for (int t = hi; t >= lo; --t) {
+    if (c.eP != 1.0) blk_scale(A, lda, c.N, c.N, c.eP);
+    build_table(c, s, t);
+    kin_rows(c, s, A, lda, c.N, 1);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Stabilization (src/stabilization.f90:42-264)
+// ---------------------------------------------------------------------------
+// stab_UR (left = false) / stab_UL (left = true).  On entry A (lda) holds the
+// propagated U (UR, or UL^T); U, D, V are the chain's factors in global
+// memory (U = UR or UL^T).  W0 is an N x N global workspace.
+__device__ __noinline__ void dev_stab_U(const Smem &s, int N, double *A, int lda, double *U, double *D,
+                           double *V, double *W0, bool left) {
+  double *tau = s.vec, *vn1 = s.vec + N, *vn2 = s.vec + 2 * N, *Dn = s.vec + 3 * N;
+  int *jpvt = s.ivec;
+  blk_scale_cols(A, lda, N, N, D);                 // matUDV(:,i) *= D(i)
+  blk_geqp3(A, lda, N, jpvt, tau, vn1, vn2);       // ZGEQP3
+  blk_qdrp_scale(A, lda, N, Dn);                   // D = |R_ii|, R rows /= D
+  for (int i = threadIdx.x; i < N; i += Z2_NT) D[i] = Dn[i];
+  __syncthreads();
+  if (!left) {
+    // VR <- R * (P^T VR)     (ZLAPMR(.true.) + ZTRMM('L','U','N','N'))
+    blk_perm_rows(W0, N, V, N, N, N, jpvt, true);
+    GemmOp op{A, lda, false, true, W0, N, false, false};
+    blk_gemm(N, N, N, 1.0, op, 0.0, V, N, s.tile);
+  } else {
+    // VL <- (VL P) R^T       (ZLAPMT(.true.) + ZTRMM('R','U','C','N'))
+    blk_perm_cols(W0, N, V, N, N, N, jpvt, true);
+    GemmOp op{W0, N, false, false, A, lda, true, true};
+    blk_gemm(N, N, N, 1.0, op, 0.0, V, N, s.tile);
+  }
+  blk_org2r(A, lda, N, N, tau);                    // ZUNGQR
+  blk_copy(U, N, A, lda, N, N);                    // UR = Q, or UL^T = Q
+}
+
+// stab_green: G = (I + UR DR VR VL DL UL)^{-1} into Gout (global, ld N).
+// M (ldm) is the QR work matrix; W1, W2, W3 are N x N global workspaces.
+__device__ __noinline__ void dev_stab_green(const Smem &s, int N, int nt, int Ltrot, const double *UR,
+                               const double *DR, const double *VR, const double *ULT,
+                               const double *DL, const double *VL, double *M, int ldm,
+                               double *W1, double *W2, double *W3, double *Gout) {
+  double *tau = s.vec, *vn1 = s.vec + N, *vn2 = s.vec + 2 * N, *Dn = s.vec + 3 * N;
+  int *jpvt = s.ivec;
+  // invULUR = UR^T UL^T ; VRVL = VR VL
+  {
+    GemmOp op{UR, N, true, false, ULT, N, false, false};
+    blk_gemm(N, N, N, 1.0, op, 0.0, M, ldm, s.tile);
+    GemmOp op2{VR, N, false, false, VL, N, false, false};
+    blk_gemm(N, N, N, 1.0, op2, 0.0, W1, N, s.tile);
+  }
+  // matUDV = invULUR + DR (VRVL DL)   (src/stabilization.f90:138-146)
+  for (int j = threadIdx.x / 32; j < N; j += Z2_WARPS) {
+    double dl = DL[j];
+    for (int i = threadIdx.x & 31; i < N; i += 32) {
+      double t = W1[i + (size_t)j * N] * dl;
+      double u = DR[i] * t;
+      M[i + (size_t)j * ldm] = M[i + (size_t)j * ldm] + u;
+    }
+  }
+  __syncthreads();
+  const int half = Ltrot / 2;
+  if (nt > half) {   // matUDV = matUDV^dagger
+    for (int e = threadIdx.x; e < N * N; e += Z2_NT) {
+      int i = e % N, j = e / N;
+      if (i < j) {
+        double a = M[i + (size_t)j * ldm], b = M[j + (size_t)i * ldm];
+        M[i + (size_t)j * ldm] = b;
+        M[j + (size_t)i * ldm] = a;
+      }
+    }
+    __syncthreads();
+  }
+  blk_geqp3(M, ldm, N, jpvt, tau, vn1, vn2);
+  blk_qdrp_scale(M, ldm, N, Dn);
+  if (nt < half + 1) {
+    // G = UL^dagger P V^-1 D^-1 U^dagger UR^dagger
+    blk_transpose(W2, N, UR, N, N, N);                     // temp = UR^T
+    blk_ormqr_LT(M, ldm, N, tau, W2, N, N);                // Q^T temp
+    for (int j = threadIdx.x / 32; j < N; j += Z2_WARPS)
+      for (int i = threadIdx.x & 31; i < N; i += 32) W2[i + (size_t)j * N] = W2[i + (size_t)j * N] / Dn[i];
+    __syncthreads();
+    blk_trsm_LUN(M, ldm, N, W2, N, N);                     // V^-1 (...)
+    blk_perm_rows(W3, N, W2, N, N, N, jpvt, false);        // ZLAPMR(.false.)
+    GemmOp op{ULT, N, false, false, W3, N, false, false};  // UL^T temp
+    blk_gemm(N, N, N, 1.0, op, 0.0, Gout, N, s.tile);
+  } else {
+    // G = UL^dagger U D^-1 V P^-1 UR^dagger
+    blk_copy(W2, N, ULT, N, N, N);                         // temp = UL^T
+    blk_ormqr_RN(M, ldm, N, tau, W2, N, N);                // temp Q
+    for (int j = threadIdx.x / 32; j < N; j += Z2_WARPS) {
+      double d = Dn[j];
+      for (int i = threadIdx.x & 31; i < N; i += 32) W2[i + (size_t)j * N] = W2[i + (size_t)j * N] / d;
+    }
+    __syncthreads();
+    blk_trsm_RUT(M, ldm, N, W2, N, N);                     // (...) V^-dagger
+    blk_perm_cols(W3, N, W2, N, N, N, jpvt, false);        // ZLAPMT(.false.)
+    GemmOp op{W3, N, false, false, UR, N, true, false};    // temp UR^T
+    blk_gemm(N, N, N, 1.0, op, 0.0, Gout, N, s.tile);
+  }
+}
+
+// stab_green_big (src/stabilization.f90:202-264): the four blocks of the
+// 2N x 2N Green's function.  Inverses of the orthogonal factors (UL UR,
+// bigU, UR, UL) are their transposes; VR VL, VR and VL are inverted by LU;
+// bigV (triangular) by a triangular solve.
+__device__ __noinline__ void dev_stab_green_big(const Smem &s, int N, const double *UR, const double *DR,
+                                   const double *VR, const double *ULT, const double *DL,
+                                   const double *VL, double *W0, double *W1, double *W2,
+                                   double *W3, double *B0, double *B1, double *B2, double *B3) {
+  const int n2 = 2 * N;
+  double *tau = s.vec;          // 2N
+  double *bigD = s.vec + 2 * N; // 2N
+  int *ipiv = s.ivec;
+  // invVRVL = (VR VL)^-1  -> W0
+  {
+    GemmOp op{VR, N, false, false, VL, N, false, false};
+    blk_gemm(N, N, N, 1.0, op, 0.0, W0, N, s.tile);
+    blk_inverse(W0, N, N, W1, N, ipiv, s.red, s.flag);
+  }
+  // invULUR = UR^T UL^T -> W1
+  {
+    GemmOp op{UR, N, true, false, ULT, N, false, false};
+    blk_gemm(N, N, N, 1.0, op, 0.0, W1, N, s.tile);
+  }
+  // big matrix
+  for (int j = threadIdx.x / 32; j < n2; j += Z2_WARPS)
+    for (int i = threadIdx.x & 31; i < n2; i += 32) {
+      double v = 0.0;
+      if (i < N && j < N) v = W0[i + (size_t)j * N];
+      else if (i >= N && j >= N) v = W1[(i - N) + (size_t)(j - N) * N];
+      else if (i < N && j == i + N) v = DL[i];
+      else if (i >= N && j == i - N) v = -DR[j];
+      B0[i + (size_t)j * n2] = v;
+    }
+  __syncthreads();
+  // UDV_C: QR, D = |R_ii|, V = R / D, determinant-sign fix
+  blk_geqr2(B0, n2, n2, n2, tau);
+  blk_copy(B1, n2, B0, n2, n2, n2);
+  blk_org2r(B1, n2, n2, n2, tau);                 // bigU
+  {
+    // sign of prod R_ii (mat_mod.f90:650-657): count negative diagonals
+    int neg = 0;
+    for (int i = threadIdx.x; i < n2; i += Z2_NT) neg += (B0[i + (size_t)i * n2] < 0.0);
+    double t = blk_sum((double)neg, s.red);
+    int flip = ((int)t) & 1;
+    for (int i = threadIdx.x; i < n2; i += Z2_NT) bigD[i] = fabs(B0[i + (size_t)i * n2]);
+    __syncthreads();
+    // bigV = R / D (upper), into B2 ; flip row 0 of V and column 0 of U if needed
+    for (int j = threadIdx.x / 32; j < n2; j += Z2_WARPS)
+      for (int i = threadIdx.x & 31; i < n2; i += 32) {
+        double v = (i <= j) ? B0[i + (size_t)j * n2] : 0.0;
+        if (flip && i == 0) v = -v;
+        B2[i + (size_t)j * n2] = v / bigD[i];
+      }
+    if (flip)
+      for (int i = threadIdx.x; i < n2; i += Z2_NT) B1[i] = -B1[i];
+    __syncthreads();
+  }
+  // invbigV: solve bigV X = I -> B3
+  blk_identity(B3, n2, n2);
+  blk_trsm_LUN(B2, n2, n2, B3, n2, n2);
+  // invVUR -> W2, invVUL -> W3
+  blk_copy(W2, N, VR, N, N, N);
+  blk_inverse(W2, N, N, W0, N, ipiv, s.red, s.flag);
+  blk_copy(W3, N, VL, N, N, N);
+  blk_inverse(W3, N, N, W0, N, ipiv, s.red, s.flag);
+  // mat_left = diag(invVUR, invUUL) invbigV -> B0
+  {
+    GemmOp op{W2, N, false, false, B3, n2, false, false};
+    blk_gemm(N, n2, N, 1.0, op, 0.0, B0, n2, s.tile);
+    GemmOp op2{ULT, N, false, false, B3 + N, n2, false, false};
+    blk_gemm(N, n2, N, 1.0, op2, 0.0, B0 + N, n2, s.tile);
+  }
+  // mat_right = invbigU diag(invVUL, invUUR) -> B2 ; invbigU = bigU^T
+  {
+    GemmOp op{B1, n2, true, false, W3, N, false, false};
+    blk_gemm(n2, N, N, 1.0, op, 0.0, B2, n2, s.tile);
+    GemmOp op2{B1 + N, n2, true, false, UR, N, true, false};
+    blk_gemm(n2, N, N, 1.0, op2, 0.0, B2 + (size_t)N * n2, n2, s.tile);
+  }
+  // mat_left(:, nr) /= bigD(nr)
+  for (int j = threadIdx.x / 32; j < n2; j += Z2_WARPS) {
+    double d = bigD[j];
+    for (int i = threadIdx.x & 31; i < n2; i += 32) B0[i + (size_t)j * n2] = B0[i + (size_t)j * n2] / d;
+  }
+  __syncthreads();
+  {
+    GemmOp op{B0, n2, false, false, B2, n2, false, false};
+    blk_gemm(n2, n2, n2, 1.0, op, 0.0, B3, n2, s.tile);
+  }
+}
+
+// Blocks of the 2N x 2N Green's function left in B3 by dev_stab_green_big.
+__device__ __noinline__ void green_big_extract(int N, const double *B3, double *G00, double *G0t,
+                                  double *Gt0, double *Gtt) {
+  const int n2 = 2 * N;
+  blk_copy(G00, N, B3, n2, N, N);
+  blk_copy(G0t, N, B3 + (size_t)N * n2, n2, N, N);
+  blk_copy(Gt0, N, B3 + N, n2, N, N);
+  blk_copy(Gtt, N, B3 + N + (size_t)N * n2, n2, N, N);
+}
+
+// ---------------------------------------------------------------------------
+// Delayed rank-2 updates (LocalK_metro, src/localK.f90:45-173)
+// ---------------------------------------------------------------------------
+// G <- G - X Yt^T over the m queued columns, 4x4 register tiles.
+__device__ __noinline__ void rank_update(double *G, int ldg, const double *X, const double *Yt, int N, int m) {
+  const int T = (N + 3) >> 2;
+  for (int t = threadIdx.x; t < T * T; t += Z2_NT) {
+    const int ti = t % T, tj = t / T;
+    double acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+    int rows[4], cols[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) { rows[a] = ti + T * a; cols[a] = 4 * tj + a; }
+    for (int q = 0; q < m; ++q) {
+      const double *xq = X + (size_t)q * N, *yq = Yt + (size_t)q * N;
+      double xa[4], yb[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) xa[a] = rows[a] < N ? xq[rows[a]] : 0.0;
+#pragma unroll
+      for (int b = 0; b < 4; ++b) yb[b] = cols[b] < N ? yq[cols[b]] : 0.0;
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = fma(xa[a], yb[b], acc[a][b]);
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+        if (rows[a] < N && cols[b] < N) G[rows[a] + (size_t)cols[b] * ldg] -= acc[a][b];
+  }
+  __syncthreads();
+}
+
+// The 2N proposals of one slice (LocalK_prop_L: bonds 2N..1, LocalK_prop_R:
+// bonds 1..2N).  Warp 0 evaluates 32 consecutive proposals speculatively
+// against the current G = G0 - X Yt^T; all proposals before the first
+// accepted one are rejections (G and sigma unchanged), so they are exact.
+// One ranf draw per proposal (src/localK.f90:123), advanced in closed form.
+__device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, int nt, bool descending,
+                              int dir) {
+  const int N = c.N, nb = c.nb, k2 = c.k2, Lt = c.Ltrot;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double *G = s.G; const int ldg = s.ldg;
+  double *X = s.X, *Yt = s.Yt;
+  signed char *sg = c.sigma + (size_t)(nt - 1) * nb;
+  const signed char *sprev = c.sigma + (size_t)((nt - 2 + Lt) % Lt) * nb;
+  const signed char *snext = c.sigma + (size_t)(nt % Lt) * nb;
+  for (int i = threadIdx.x; i < nb; i += Z2_NT) s.sig[i] = sg[i];
+  __syncthreads();
+  double *pdat = s.red + 48;      // accepted proposal: pinv(4), D11, D12
+  int m = 0, done = 0;
+  while (done < nb) {
+    if (warp == 0) {
+      const int kk = done + lane;
+      const bool valid = kk < nb;
+      const int b = valid ? (descending ? nb - 1 - kk : kk) : 0;
+      const int p1 = s.bond[2 * b], p2 = s.bond[2 * b + 1];
+      double g11 = G[p1 + (size_t)p1 * ldg], g12 = G[p1 + (size_t)p2 * ldg];
+      double g21 = G[p2 + (size_t)p1 * ldg], g22 = G[p2 + (size_t)p2 * ldg];
+      for (int q = 0; q < m; ++q) {
+        double xa = X[p1 + (size_t)q * N], xb = X[p2 + (size_t)q * N];
+        double ya = Yt[p1 + (size_t)q * N], yb = Yt[p2 + (size_t)q * N];
+        g11 -= xa * ya; g12 -= xa * yb; g21 -= xb * ya; g22 -= xb * yb;
+      }
+      const double s_old = (double)s.sig[b];
+      const double s_new = -s_old;
+      const double D11 = c.dlt[2 * b], D12 = s_new * c.dlt[2 * b + 1];
+      // (I - G)_PP, Prod = I + Delta (I - G)_PP, determinant (no FMA
+      // contraction: same rounding sequence as the reference)
+      const double l11 = __dsub_rn(1.0, g11), l12 = -g12, l21 = -g21, l22 = __dsub_rn(1.0, g22);
+      const double m11 = __dadd_rn(__dmul_rn(D11, l11), __dmul_rn(D12, l21));
+      const double m12 = __dadd_rn(__dmul_rn(D11, l12), __dmul_rn(D12, l22));
+      const double m21 = __dadd_rn(__dmul_rn(D12, l11), __dmul_rn(D11, l21));
+      const double m22 = __dadd_rn(__dmul_rn(D12, l12), __dmul_rn(D11, l22));
+      const double p11 = __dadd_rn(1.0, m11), p12 = m12, p21 = m21, p22 = __dadd_rn(1.0, m22);
+      const double det = __dsub_rn(__dmul_rn(p11, p22), __dmul_rn(p12, p21));
+      // boson ratio (src/fields.f90:40-119) from the host table
+      const int *bb = c.bbonds + 6 * b;
+      const double tmp_old = s_old * s.sig[bb[0]] * s.sig[bb[1]] * s.sig[bb[2]] +
+                             s_old * s.sig[bb[3]] * s.sig[bb[4]] * s.sig[bb[5]];
+      const int is = (int)(-2.0 * tmp_old + 4.0) >> 2;
+      const double tn = s_old * ((double)sprev[b] + (double)snext[b]);
+      const int it = (int)(-2.0 * tn + 4.0) >> 2;
+      const double ratio = __dmul_rn(__dmul_rn(det, det), c.rb[is * 3 + it]);
+      // uniform: replayed or ranf
+      const unsigned int st = *c.rng;
+      long long rpos = c.replay ? *c.replay_pos : 0;
+      double r;
+      if (c.replay && rpos + lane < c.nreplay) r = c.replay[rpos + lane];
+      else r = (double)ranf_adv(st, lane + 1) * (1.0 / 2147483648.0);
+      const bool acc = valid && (fabs(ratio) > r);
+      const unsigned ball = __ballot_sync(Z2_FULL, acc);
+      const int first = ball ? (__ffs(ball) - 1) : 32;
+      const int rem = nb - done;
+      const int cnt = (first < 32) ? first + 1 : (rem < 32 ? rem : 32);
+      if (lane < cnt && c.dec) {
+        size_t li = ((size_t)dir * Lt + (nt - 1)) * nb + b;
+        c.dec[li] = (lane == first) ? 1 : 0;
+        if (c.ratios) c.ratios[li] = ratio;
+      }
+      if (lane == first) {
+        const double inv = 1.0 / det;
+        pdat[0] = p22 / det; pdat[1] = -p12 / det; pdat[2] = -p21 / det; pdat[3] = p11 / det;
+        (void)inv;
+        pdat[4] = D11; pdat[5] = D12;
+        s.flag[1] = b;
+      }
+      __syncwarp();
+      if (lane == 0) {
+        s.flag[0] = done + cnt;
+        if (first == 32) s.flag[1] = -1;
+        *c.rng = ranf_adv(st, cnt);
+        if (c.replay) *c.replay_pos = rpos + cnt;
+        c.acc[A_ACC_DEN] += (double)cnt;
+        c.acc[A_DRAWS] += (double)cnt;
+        if (first < 32) c.acc[A_ACC_NUM] += 1.0;
+      }
+    }
+    __syncthreads();
+    done = s.flag[0];
+    const int b = s.flag[1];
+    if (b >= 0) {
+      const int p1 = s.bond[2 * b], p2 = s.bond[2 * b + 1];
+      const double q00 = pdat[0], q01 = pdat[1], q10 = pdat[2], q11 = pdat[3];
+      const double D11 = pdat[4], D12 = pdat[5];
+      for (int i = threadIdx.x; i < N; i += Z2_NT) {
+        double u0 = G[i + (size_t)p1 * ldg], u1 = G[i + (size_t)p2 * ldg];
+        double v0 = G[p1 + (size_t)i * ldg], v1 = G[p2 + (size_t)i * ldg];
+        for (int q = 0; q < m; ++q) {
+          const double xi = X[i + (size_t)q * N], yi = Yt[i + (size_t)q * N];
+          u0 -= xi * Yt[p1 + (size_t)q * N];
+          u1 -= xi * Yt[p2 + (size_t)q * N];
+          v0 -= X[p1 + (size_t)q * N] * yi;
+          v1 -= X[p2 + (size_t)q * N] * yi;
+        }
+        // temp = Uhlp * Prodinv ; Vhlp = Delta (I - G)(P, :)
+        X[i + (size_t)m * N] = u0 * q00 + u1 * q10;
+        X[i + (size_t)(m + 1) * N] = u0 * q01 + u1 * q11;
+        double y0 = -D11 * v0 - D12 * v1;
+        double y1 = -D12 * v0 - D11 * v1;
+        if (i == p1) { y0 += D11; y1 += D12; }
+        if (i == p2) { y0 += D12; y1 += D11; }
+        Yt[i + (size_t)m * N] = y0;
+        Yt[i + (size_t)(m + 1) * N] = y1;
+      }
+      if (threadIdx.x == 0) {
+        signed char sn = (signed char)(-s.sig[b]);
+        s.sig[b] = sn;
+        sg[b] = sn;
+      }
+      __syncthreads();
+      m += 2;
+      if (m >= k2) { rank_update(G, ldg, X, Yt, N, m); m = 0; }
+    }
+  }
+  if (m > 0) rank_update(G, ldg, X, Yt, N, m);
+}
+
+// ---------------------------------------------------------------------------
+// Equal-time observables (Obs_equal_calc, src/obser_equal.f90:73-149)
+// ---------------------------------------------------------------------------
+__device__ __noinline__ void obs_equal(const ChainDesc &c, const Smem &s, int nt) {
+  const int N = c.N;
+  const double *G = s.G; const int ldg = s.ldg;
+  const signed char *sg = c.sigma + (size_t)(nt - 1) * c.nb;
+  double v[5] = {0, 0, 0, 0, 0};   // flux, pair, cdw, cdw_shift, density
+  for (int i = threadIdx.x; i < N; i += Z2_NT) {
+    const int *pl = c.plaq + 4 * i;
+    v[0] += (double)sg[pl[0]] * (double)sg[pl[1]] * (double)sg[pl[2]] * (double)sg[pl[3]];
+    double n = 1.0 - G[i + (size_t)i * ldg];
+    v[4] += n + n;
+  }
+  const int W = 2 * c.Lx - 1;
+  for (int e = threadIdx.x; e < N * N; e += Z2_NT) {
+    const int i = e % N, j = e / N;
+    const double gij = G[i + (size_t)j * ldg], gji = G[j + (size_t)i * ldg];
+    const double ni = 1.0 - G[i + (size_t)i * ldg], nj = 1.0 - G[j + (size_t)j * ldg];
+    const double dl = (i == j) ? 1.0 : 0.0;
+    const double pq = dl - gij;
+    v[1] += pq * pq;
+    const double a = ni * nj;
+    const double ex = (dl - gji) * gij;
+    double dc = a - ex;
+    dc = (dc + a) - ex;
+    dc = (dc + a) + a;
+    const double ph = c.stag[i] * c.stag[j];
+    const int dx = c.xy[2 * i] - c.xy[2 * j], dy = c.xy[2 * i + 1] - c.xy[2 * j + 1];
+    const double ps = c.pshift[(dx + c.Lx - 1) + (dy + c.Ly - 1) * W];
+    v[2] += ph * dc;
+    v[3] += ps * dc;
+  }
+  blk_sum_n<5>(v, s.red);
+  if (threadIdx.x == 0) {
+    const double flux = v[0] / (double)N;
+    c.acc[A_FLUX_SUM] += flux;
+    c.acc[A_FLUX_SQ] += flux * flux;
+    c.acc[A_PAIR] += v[1];
+    c.acc[A_CDW] += v[2];
+    c.acc[A_CDWS] += v[3];
+    c.acc[A_DENS] += v[4] / (double)N;
+    c.acc[A_NOBS] += 1.0;
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// Time-displaced observables (Obs_tau_calc, src/obser_tau.f90:56-133), real
+// parts, both identical spin sectors summed; binned by imj deterministically
+// (one thread per displacement).
+// ---------------------------------------------------------------------------
+__device__ __noinline__ void obs_tau(const ChainDesc &c, const Smem &s, int nt) {
+  const int N = c.N, Lx = c.Lx, Ly = c.Ly;
+  const double *G00 = c.G00, *Gtt = c.Gtt, *Gt0 = c.Gt0, *G0t = c.G0t;
+  const signed char *sgt = c.sigma + (size_t)(nt - 1) * c.nb;
+  const signed char *sg1 = c.sigma;
+  const double rt2 = c.rt_scalar * c.rt_scalar;
+  for (int r = threadIdx.x; r < N; r += Z2_NT) {
+    const int rx = c.xy[2 * r], ry = c.xy[2 * r + 1];
+    double o[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int ii = 0; ii < N; ++ii) {
+      const int ix = c.xy[2 * ii], iy = c.xy[2 * ii + 1];
+      int jx = ix - rx; if (jx < 1) jx += Lx;
+      int jy = iy - ry; if (jy < 1) jy += Ly;
+      const int jj = (jy - 1) * Lx + (jx - 1);
+      const int ip = c.nbx[ii], jp = c.nbx[jj];
+      // spin: sigma(ii, ntau) * sigma(jj, 1)
+      o[0] += (double)sgt[ii] * (double)sg1[jj];
+      const double g0t_ji = G0t[jj + (size_t)ii * N];
+      const double gt0_ij = Gt0[ii + (size_t)jj * N];
+      // single: term = Grt0u + Grt0d ; += term + conj(term)
+      const double term = gt0_ij + gt0_ij;
+      o[1] += term + term;
+      // pair_d / pair_s: (diag1 + diag2) * 4
+      const double d1 = g0t_ji * g0t_ji;
+      const double pr = (d1 + d1) * 4.0;
+      o[2] += pr;
+      o[3] += pr;
+      // charge: -Gr0t(jj,ii) Grt0(ii,jj) - conj(...) for both spins
+      const double y = g0t_ji * gt0_ij;
+      const double tt = 2.0 * (1.0 - Gtt[ii + (size_t)ii * N]);
+      const double t0 = 2.0 * (1.0 - G00[jj + (size_t)jj * N]);
+      const double chc = ((-y - y) - y) - y;
+      o[4] += chc + (tt - tt) * (t0 - t0);
+      o[5] += chc + (tt + tt) * (t0 + t0);
+      // curxx with NB_field = 0
+      const double tc = -G0t[jj + (size_t)ip * N] * Gt0[ii + (size_t)jp * N]
+                        - G0t[jp + (size_t)ii * N] * Gt0[ip + (size_t)jj * N]
+                        + G0t[jj + (size_t)ii * N] * Gt0[ip + (size_t)jp * N]
+                        + G0t[jp + (size_t)ip * N] * Gt0[ii + (size_t)jj * N];
+      const double cu = -rt2 * tc - rt2 * tc;
+      o[6] += cu + cu;
+    }
+    double *ot = c.obs_tau + (size_t)(nt - 1) * N + r;
+#pragma unroll
+    for (int q = 0; q < 7; ++q) ot[(size_t)q * c.Ltrot * N] += o[q];
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// Wraps (src/stabilization.f90:374-514)
+// ---------------------------------------------------------------------------
+struct Pend { int lo, hi; };   // lazily propagated slices, lo > hi = none
+
+__device__ __forceinline__ double *qr_matrix(const ChainDesc &c, const Smem &s, int &ld) {
+  ld = s.ldq;
+  return s.Wq;
+}
+
+__device__ __noinline__ void spill_G(const ChainDesc &c, const Smem &s) {
+  if (c.g_in_smem) blk_copy(c.G, c.N, s.G, s.ldg, c.N, c.N);
+}
+__device__ __noinline__ void load_G(const ChainDesc &c, const Smem &s) {
+  if (c.g_in_smem) blk_copy(s.G, s.ldg, c.G, c.N, c.N, c.N);
+}
+
+__device__ __noinline__ void copy_vec(double *dst, const double *src, int n) {
+  for (int i = threadIdx.x; i < n; i += Z2_NT) dst[i] = src[i];
+  __syncthreads();
+}
+
+__device__ __noinline__ void record_drift(const ChainDesc &c, double dif, bool stats) {
+  if (threadIdx.x == 0) {
+    if (dif > c.acc[A_XMAX] || dif != dif) c.acc[A_XMAX] = dif;
+    if (stats) c.acc[A_XMEAN] += dif;
+    if (!(dif == dif) || isinf(dif)) atomicOr(c.status, ST_NONFINITE);
+  }
+}
+
+// Wrap_pre (src/stabilization.f90:374-398)
+__device__ __noinline__ void wrap_pre(const ChainDesc &c, const Smem &s, int nt, Pend &pd) {
+  const int N = c.N, NN = N * N;
+  int lda; double *A = qr_matrix(c, s, lda);
+  const int st = nt / c.Nwrap;
+  if (nt != 0) {
+    blk_copy(A, lda, c.UR, N, N, N);
+    apply_pending_R(c, s, A, lda, pd.lo, pd.hi, c.use_kin != 0);
+    dev_stab_U(s, N, A, lda, c.UR, c.DR, c.VR, c.W0, false);
+  }
+  pd.lo = 1; pd.hi = 0;
+  blk_copy(c.URs + (size_t)st * NN, N, c.UR, N, N, N);
+  blk_copy(c.VRs + (size_t)st * NN, N, c.VR, N, N, N);
+  copy_vec(c.DRs + (size_t)st * N, c.DR, N);
+  if (nt == c.Ltrot) {
+    dev_stab_green(s, N, nt, c.Ltrot, c.UR, c.DR, c.VR, c.ULT, c.DL, c.VL, A, lda, c.W1, c.W2,
+                   c.W0, c.G);
+  }
+}
+
+// Wrap_L (src/stabilization.f90:400-437)
+__device__ __noinline__ void wrap_L(const ChainDesc &c, const Smem &s, int nt, Pend &pd, bool stats) {
+  const int N = c.N, NN = N * N;
+  spill_G(c, s);
+  int lda; double *A = qr_matrix(c, s, lda);
+  const int st = nt / c.Nwrap;
+  blk_copy(c.UR, N, c.URs + (size_t)st * NN, N, N, N);
+  blk_copy(c.VR, N, c.VRs + (size_t)st * NN, N, N, N);
+  copy_vec(c.DR, c.DRs + (size_t)st * N, N);
+  if (pd.lo <= pd.hi) {
+    blk_copy(A, lda, c.ULT, N, N, N);
+    apply_pending_L(c, s, A, lda, pd.lo, pd.hi);
+    if (nt == c.Ltrot) blk_copy(c.ULT, N, A, lda, N, N);
+  } else if (nt != c.Ltrot) {
+    blk_copy(A, lda, c.ULT, N, N, N);
+  }
+  pd.lo = 1; pd.hi = 0;
+  if (nt != c.Ltrot) {
+    dev_stab_U(s, N, A, lda, c.ULT, c.DL, c.VL, c.W0, true);
+    dev_stab_green(s, N, nt, c.Ltrot, c.UR, c.DR, c.VR, c.ULT, c.DL, c.VL, A, lda, c.W1, c.W2,
+                   c.W0, c.W3);
+    double dif = blk_maxdiff(c.W3, N, c.G, N, N, s.red);
+    record_drift(c, dif, stats);
+    blk_copy(c.G, N, c.W3, N, N, N);
+  }
+  blk_copy(c.ULTs + (size_t)st * NN, N, c.ULT, N, N, N);
+  blk_copy(c.VLs + (size_t)st * NN, N, c.VL, N, N, N);
+  copy_vec(c.DLs + (size_t)st * N, c.DL, N);
+  load_G(c, s);
+}
+
+// Wrap_R (src/stabilization.f90:439-476)
+__device__ __noinline__ void wrap_R(const ChainDesc &c, const Smem &s, int nt, Pend &pd, bool stats) {
+  const int N = c.N, NN = N * N;
+  spill_G(c, s);
+  int lda; double *A = qr_matrix(c, s, lda);
+  const int st = nt / c.Nwrap;
+  blk_copy(c.ULT, N, c.ULTs + (size_t)st * NN, N, N, N);
+  blk_copy(c.VL, N, c.VLs + (size_t)st * NN, N, N, N);
+  copy_vec(c.DL, c.DLs + (size_t)st * N, N);
+  if (pd.lo <= pd.hi) {
+    blk_copy(A, lda, c.UR, N, N, N);
+    apply_pending_R(c, s, A, lda, pd.lo, pd.hi, true);
+    if (nt == 0) blk_copy(c.UR, N, A, lda, N, N);
+  } else if (nt != 0) {
+    blk_copy(A, lda, c.UR, N, N, N);
+  }
+  pd.lo = 1; pd.hi = 0;
+  if (nt != 0) {
+    dev_stab_U(s, N, A, lda, c.UR, c.DR, c.VR, c.W0, false);
+    dev_stab_green(s, N, nt, c.Ltrot, c.UR, c.DR, c.VR, c.ULT, c.DL, c.VL, A, lda, c.W1, c.W2,
+                   c.W0, c.W3);
+    double dif = blk_maxdiff(c.W3, N, c.G, N, N, s.red);
+    record_drift(c, dif, stats);
+    blk_copy(c.G, N, c.W3, N, N, N);
+  }
+  blk_copy(c.URs + (size_t)st * NN, N, c.UR, N, N, N);
+  blk_copy(c.VRs + (size_t)st * NN, N, c.VR, N, N, N);
+  copy_vec(c.DRs + (size_t)st * N, c.DR, N);
+  load_G(c, s);
+}
+
