@@ -27,11 +27,12 @@ the reference project root).  Numerics:
   give the same Green's functions to rounding because the time-displaced
   Green's function does not depend on the QR convention.
 
-Parity status: the reference cannot be compiled here (no Fortran compiler,
-no MPI) and ships no golden vectors, so this oracle is pinned by known-answer
-tests (RNG closed form, free-fermion limit, dense-product Green's function,
-mu-derivative identity, complex/real agreement) rather than by reference
-outputs; see tests/test_oracle.py.
+Parity status: parity unpinned.  The reference cannot be compiled here (no
+Fortran compiler, no MPI) and its tests hold no golden vectors for this path,
+so the oracle is not checked against reference outputs.  What pins it instead
+are known-answer tests built from the algorithm itself (ranf closed form,
+free-fermion limit, dense-product Green's function, mu-derivative identity,
+complex/real agreement, lattice invariants); see tests/test_oracle.py.
 """
 from __future__ import annotations
 
