@@ -139,6 +139,27 @@ int z2_stab_green_big(z2_handle *h, int32_t chain, const double *UR,
                       const double *DL, const double *VL, double *G00,
                       double *G0t, double *Gt0, double *Gtt);
 
+/* ---- allocation-free stab_green.  No counterpart in the reference.
+ * For callers that cannot call cudaMalloc (their device memory is owned by
+ * another allocator, e.g. a framework's caching allocator or a driver that
+ * reserves one pool at start-up): same result as z2_stab_green, but UR, DR,
+ * VR, UL, DL, VL (inputs) and G (output) are caller-owned DEVICE pointers,
+ * column-major N x N (DR, DL of length N), and no memory is allocated.  The
+ * scratch is a file-scope device array of 5 * Z2_NOALLOC_NMAX^2 doubles
+ * (829,440 bytes) that every GPU loading this library holds until exit.
+ * N > Z2_NOALLOC_NMAX (or N < 1, nt outside 0..Ltrot, a null pointer) is
+ * rejected with Z2_ERR_ARG.  The work is enqueued on `stream` (a
+ * cudaStream_t, NULL = default stream); the call returns after the launch.
+ * The first call on a device looks up the device address of the scratch
+ * array (cudaGetSymbolAddress) with that device current; make that first
+ * call before any stream capture.  Every call shares the one scratch array,
+ * so calls that overlap on the GPU (other streams, other host threads) race;
+ * no part of the scratch needs to start at zero. ---- */
+#define Z2_NOALLOC_NMAX 144
+int z2_stab_green_noalloc(int32_t N, int32_t nt, int32_t Ltrot, const double *UR,
+                          const double *DR, const double *VR, const double *UL,
+                          const double *DL, const double *VL, double *G, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -888,3 +888,77 @@ extern "C" int z2_stab_green_big(z2_handle *h, int32_t chain, const double *UR, 
   CUDA_TRY(h, cudaMemcpy(Gtt, a.Gtt, NN * 8, cudaMemcpyDeviceToHost));
   return Z2_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free stab_green.
+//
+// Some callers cannot call cudaMalloc: for instance a host program whose
+// device memory is owned by another allocator (a framework's caching
+// allocator, or a Fortran driver that reserves one pool at start-up and
+// forbids further driver allocations inside its time-stepping loop).  For
+// them this entry point computes the same Green's function as z2_stab_green,
+// with caller-owned device buffers for inputs and outputs and its scratch in
+// the file-scope array below, which every GPU that loads this library keeps
+// until the process exits: 5 * Z2_NOALLOC_NMAX^2 doubles (829,440 bytes).
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+static __device__ __align__(256) double z2_noalloc_scratch[5 * Z2_NOALLOC_NMAX * Z2_NOALLOC_NMAX];
+
+__global__ void __launch_bounds__(Z2_NT, 1)
+z2_stab_green_noalloc_kernel(int N, int nt, int Ltrot, const double *UR, const double *DR,
+                             const double *VR, const double *UL, const double *DL,
+                             const double *VL, double *G, double *scratch) {
+  extern __shared__ __align__(16) unsigned char z2_smem[];
+  Smem s{};
+  size_t off = 0;
+  s.red = (double *)(z2_smem + off); off += sizeof(double) * Z2_NRED;
+  s.vec = (double *)(z2_smem + off); off += sizeof(double) * 8 * N;
+  s.ivec = (int *)(z2_smem + off); off += align16(sizeof(int) * 2 * N);
+  s.flag = (int *)(z2_smem + off); off += sizeof(int) * 16;
+  off = align16(off);
+  s.tile = (double *)(z2_smem + off);
+  // scratch: M (QR work matrix), W1, W2, W3, UL^T; every entry read is
+  // written first by this call, so nothing has to start at zero.
+  const size_t NN = (size_t)N * N;
+  double *M = scratch, *W1 = M + NN, *W2 = W1 + NN, *W3 = W2 + NN, *ULT = W3 + NN;
+  blk_transpose(ULT, N, UL, N, N, N);
+  dev_stab_green(s, N, nt, Ltrot, UR, DR, VR, ULT, DL, VL, M, N, W1, W2, W3, G);
+}
+
+static size_t noalloc_smem_bytes(int N) {
+  size_t off = sizeof(double) * Z2_NRED + sizeof(double) * 8 * (size_t)N;
+  off += ((sizeof(int) * 2 * (size_t)N) + 15) & ~size_t(15);
+  off += sizeof(int) * 16;
+  off = (off + 15) & ~size_t(15);
+  return off + sizeof(double) * kGemmTile;
+}
+
+extern "C" int z2_stab_green_noalloc(int32_t N, int32_t nt, int32_t Ltrot, const double *UR,
+                                     const double *DR, const double *VR, const double *UL,
+                                     const double *DL, const double *VL, double *G,
+                                     void *stream) {
+  if (N < 1 || N > Z2_NOALLOC_NMAX) return Z2_ERR_ARG;
+  if (Ltrot < 1 || nt < 0 || nt > Ltrot) return Z2_ERR_ARG;
+  if (!UR || !DR || !VR || !UL || !DL || !VL || !G) return Z2_ERR_ARG;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return Z2_ERR_CUDA;
+  // Set-up, once per device with that device current: the device address of
+  // the scratch array (host code must not use the symbol itself).
+  static std::mutex mu;
+  static double *scratch_of[64] = {nullptr};
+  double *scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (!scratch_of[dev]) {
+      void *p = nullptr;
+      if (cudaGetSymbolAddress(&p, z2_noalloc_scratch) != cudaSuccess || !p) return Z2_ERR_CUDA;
+      scratch_of[dev] = (double *)p;
+    }
+    scratch = scratch_of[dev];
+  }
+  z2_stab_green_noalloc_kernel<<<1, Z2_NT, noalloc_smem_bytes(N), (cudaStream_t)stream>>>(
+      N, nt, Ltrot, UR, DR, VR, UL, DL, VL, G, scratch);
+  if (cudaGetLastError() != cudaSuccess) return Z2_ERR_CUDA;
+  return Z2_OK;
+}
