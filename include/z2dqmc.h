@@ -112,6 +112,13 @@ int z2_get_stats(const z2_handle *h, int32_t chain, double out[Z2_NSTATS]);
  * restores ranf).  Decisions/ratios of the last half-sweeps, in the order
  * (half-sweep L then R, slice nt = 1..Ltrot, bond 0..2N-1). */
 int z2_set_replay(z2_handle *h, int32_t chain, const double *r, size_t n);
+/* Tracing: SM clock cycles spent by the chain's CTA in each phase since
+ * z2_create, accumulated over all z2_sweep calls (no reference counterpart;
+ * the reference only records total wall time, src/main.f90:27-28,114-122).
+ * out[Z2_NPHASE]: checkerboard wrap of G, proposals, rank-2k flushes,
+ * equal-time observables, wraps + stabilization, time-displaced chain. */
+#define Z2_NPHASE 8
+int z2_get_phase_cycles(const z2_handle *h, int32_t chain, double out[Z2_NPHASE]);
 int z2_get_decisions(const z2_handle *h, int32_t chain, uint8_t *dec,
                      double *ratios, size_t n);
 

@@ -26,6 +26,7 @@ from ._ffi import ChainParams, Options, Z2Error, dptr, fmat
 OBS_EQ_NAMES = ("flux_avg", "chi_flux", "pair_sc_q0", "cdw_pi", "cdw_shift", "cdw_ratio",
                 "density")
 OBS_TAU_NAMES = ("spin", "single", "pair_d", "pair_s", "charge_d", "charge_s", "curxx")
+PHASE_NAMES = ("kin", "propose", "flush", "obs_equal", "wrap_stab", "dyn", "stab_U", "stab_green")
 STAT_NAMES = ("acc", "Xmaxm", "Xmeanm", "Xmaxm_tau0", "Xmaxm_tau1", "Xmaxm_tau2",
               "Xmeanm_tau0", "Xmeanm_tau1", "Xmeanm_tau2", "accepted", "proposed", "draws",
               "nobs", "nobst")
@@ -170,6 +171,12 @@ class Z2Batch:
         buf = np.empty(_ffi.Z2_NSTATS)
         self._c(self.lib.z2_get_stats(self.h, chain, dptr(buf)))
         return dict(zip(STAT_NAMES, buf.tolist()))
+
+    def phase_cycles(self, chain: int) -> dict:
+        """SM cycles per phase accumulated since creation (tracing)."""
+        buf = np.empty(8)
+        self._c(self.lib.z2_get_phase_cycles(self.h, chain, dptr(buf)))
+        return dict(zip(PHASE_NAMES, buf.tolist()))
 
     def set_replay(self, chain: int, values):
         v = np.ascontiguousarray(values, dtype=np.float64)

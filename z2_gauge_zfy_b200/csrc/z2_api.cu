@@ -274,7 +274,7 @@ static int smem_small_bytes(int N) {
   auto a16 = [](size_t x) { return (x + 15) & ~size_t(15); };
   off += 8 * Z2_NRED; off += 8 * 8 * N; off += 8 * 2 * N; off += 8 * 2 * N;
   off += a16(4 * 2 * N); off += a16(4 * 4 * N); off += a16(4 * 4 * N); off += 4 * 16;
-  off += a16(2 * N);
+  off += a16(6 * N);
   return (int)a16(off);
 }
 
@@ -331,16 +331,16 @@ extern "C" int z2_create(z2_handle **out, const z2_chain_params *params, int32_t
     size_t nn = (size_t)N * ldg;
     int g_in = 0;
     int k2 = 2 * k;
-    if (nn + std::max<size_t>(2 * (size_t)N * k2, kGemmTile) <= arena) g_in = 1;
-    else if (nn + std::max<size_t>(2 * (size_t)N * 4, kGemmTile) <= arena) {
+    if (nn + std::max<size_t>(2 * (size_t)(N | 1) * k2, kGemmTile) <= arena) g_in = 1;
+    else if (nn + std::max<size_t>(2 * (size_t)(N | 1) * 4, kGemmTile) <= arena) {
       g_in = 1;
-      while (k2 > 4 && nn + 2 * (size_t)N * k2 > arena) k2 -= 2;
+      while (k2 > 4 && nn + 2 * (size_t)(N | 1) * k2 > arena) k2 -= 2;
     }
     if (!g_in) {
-      while (k2 > 2 && 2 * (size_t)N * k2 > arena) k2 -= 2;
+      while (k2 > 2 && 2 * (size_t)(N | 1) * k2 > arena) k2 -= 2;
     }
-    size_t need = small + 8 * (g_in ? nn + std::max<size_t>(2 * (size_t)N * k2, kGemmTile)
-                                    : std::max<size_t>(2 * (size_t)N * k2, kGemmTile));
+    size_t need = small + 8 * (g_in ? nn + std::max<size_t>(2 * (size_t)(N | 1) * k2, kGemmTile)
+                                    : std::max<size_t>(2 * (size_t)(N | 1) * k2, kGemmTile));
     smem_needed = std::max(smem_needed, (int)need);
     C.d = ChainDesc{};
     C.d.N = N; C.d.Lx = p.Nlx; C.d.Ly = p.Nly; C.d.Ltrot = p.Ltrot; C.d.Nwrap = p.Nwrap;
@@ -356,7 +356,7 @@ extern "C" int z2_create(z2_handle **out, const z2_chain_params *params, int32_t
     const int N = C.N;
     size_t arena = (h->smem - smem_small_bytes(N)) / 8;
     size_t nn = (size_t)N * C.d.ldg;
-    if (C.d.g_in_smem && nn + std::max<size_t>(2 * (size_t)N * C.d.k2, kGemmTile) > arena)
+    if (C.d.g_in_smem && nn + std::max<size_t>(2 * (size_t)(N | 1) * C.d.k2, kGemmTile) > arena)
       C.d.g_in_smem = 0;
   }
   CUDA_TRY(h, cudaFuncSetAttribute(z2_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -683,6 +683,16 @@ extern "C" int z2_get_stats(const z2_handle *h, int32_t chain, double out[Z2_NST
   out[6] = a[A_TXMEAN0]; out[7] = a[A_TXMEAN1]; out[8] = a[A_TXMEAN2];
   out[9] = a[A_ACC_NUM]; out[10] = a[A_ACC_DEN]; out[11] = a[A_DRAWS];
   out[12] = a[A_NOBS]; out[13] = a[A_NOBST];
+  return Z2_OK;
+}
+
+extern "C" int z2_get_phase_cycles(const z2_handle *h, int32_t chain, double out[Z2_NPHASE]) {
+  int r = check_chain(h, chain);
+  if (r) return r;
+  z2_handle *hh = const_cast<z2_handle *>(h);
+  CUDA_TRY(hh, cudaSetDevice(h->device));
+  CUDA_TRY(hh, cudaMemcpy(out, h->ch[chain].d.acc + A_PH0, sizeof(double) * Z2_NPHASE,
+                          cudaMemcpyDeviceToHost));
   return Z2_OK;
 }
 

@@ -9,7 +9,7 @@
 // update, and the U factors of the UDV chains are propagated lazily (all
 // Nwrap slices at once, right before the stabilization that needs them).
 #pragma once
-#include "z2_linalg.cuh"
+#include "z2_stab.cuh"
 
 // Checkerboard group order of one B (src/operator_kin.f90:74-85).
 __device__ __constant__ int c_gorder[8] = {0, 1, 2, 3, 3, 2, 1, 0};
@@ -31,20 +31,20 @@ __device__ Smem make_smem(const ChainDesc &c, unsigned char *base, size_t smem_b
   s.tp = (int *)(base + off); off += align16(sizeof(int) * 4 * N);
   s.bond = (int *)(base + off); off += align16(sizeof(int) * 4 * N);
   s.flag = (int *)(base + off); off += sizeof(int) * 16;
-  s.sig = (signed char *)(base + off); off += align16(2 * N);
+  s.sig = (signed char *)(base + off); off += align16(6 * N);   // slices nt, nt-1, nt+1
   off = align16(off);
   s.arena = (double *)(base + off);
   const size_t arena_doubles = (smem_bytes - off) / sizeof(double);
   const size_t nn = (size_t)N * c.ldg;
   if (c.g_in_smem) {
     s.G = s.arena; s.ldg = c.ldg;
-    s.X = s.arena + nn; s.Yt = s.X + (size_t)N * c.k2;
+    s.ldx = N | 1; s.X = s.arena + nn; s.Yt = s.X + (size_t)s.ldx * c.k2;
     s.Wq = s.arena; s.ldq = c.ldg;
     s.tile = s.arena + nn;
     s.tile_doubles = (int)(arena_doubles - nn);
   } else {
     s.G = c.G; s.ldg = N;
-    s.X = s.arena; s.Yt = s.X + (size_t)N * c.k2;
+    s.ldx = N | 1; s.X = s.arena; s.Yt = s.X + (size_t)s.ldx * c.k2;
     s.Wq = c.W4;
     s.ldq = N;
     s.tile = s.arena;
@@ -70,78 +70,80 @@ __device__ __noinline__ void build_table(const ChainDesc &c, const Smem &s, int 
 }
 
 // M <- B^nflag M : rows P1, P2 rotated by [[C,S],[S,C]] (process_group).
-__device__ __noinline__ void kin_rows(const ChainDesc &c, const Smem &s, double *M, int ld, int ncols,
-                         int nflag) {
-  const int half = c.half;
-  const int work = half * ncols;
-  const double fl = (double)nflag;
-  for (int p = 0; p < 8; ++p) {
-    const int g0 = c_gorder[p] * half;
-    for (int idx = threadIdx.x; idx < work; idx += Z2_NT) {
-      int kq = idx / ncols;
-      int col = idx - kq * ncols;
-      int q = g0 + kq;
-      int p1 = s.tp[2 * q], p2 = s.tp[2 * q + 1];
-      double C = s.tc[q], S = fl * s.ts[q];
-      double *mc = M + (size_t)col * ld;
-      double a = mc[p1], b = mc[p2];
-      mc[p1] = C * a + S * b;
-      mc[p2] = S * a + C * b;
+// Row rotations never mix columns, so one thread carries its column through
+// all eight group passes: no barrier between passes.
+// Bonds of one group are disjoint, so a batch of 8 rotations is loaded,
+// rotated and stored as a whole (no store-to-load ordering inside a batch).
+template <bool ROWS>
+__device__ __forceinline__ void kin_group_vec(const Smem &s, double *base, size_t stride, int g0,
+                                              int half, double fl) {
+  const int2 *tp2 = reinterpret_cast<const int2 *>(s.tp);
+  int kq = 0;
+  for (; kq + 7 < half; kq += 8) {
+    int2 pp[8];
+    double C[8], S[8], a[8], b[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      pp[q] = tp2[g0 + kq + q];
+      C[q] = s.tc[g0 + kq + q];
+      S[q] = fl * s.ts[g0 + kq + q];
     }
-    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 8; ++q) { a[q] = base[pp[q].x * stride]; b[q] = base[pp[q].y * stride]; }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      base[pp[q].x * stride] = C[q] * a[q] + S[q] * b[q];
+      base[pp[q].y * stride] = S[q] * a[q] + C[q] * b[q];
+    }
+  }
+  for (; kq < half; ++kq) {
+    const int2 pp = tp2[g0 + kq];
+    const double C = s.tc[g0 + kq], S = fl * s.ts[g0 + kq];
+    const double a = base[pp.x * stride], b = base[pp.y * stride];
+    base[pp.x * stride] = C * a + S * b;
+    base[pp.y * stride] = S * a + C * b;
   }
 }
 
-// M <- M B^nflag : columns P1, P2 rotated (process_group_L).
+__device__ __noinline__ void kin_rows(const ChainDesc &c, const Smem &s, double *M, int ld, int ncols,
+                         int nflag) {
+  const int half = c.half;
+  const double fl = (double)nflag;
+  for (int col = threadIdx.x; col < ncols; col += Z2_NT) {
+    double *mc = M + (size_t)col * ld;
+    for (int p = 0; p < 8; ++p) kin_group_vec<true>(s, mc, 1, c_gorder[p] * half, half, fl);
+  }
+  __syncthreads();
+}
+
+// M <- M B^nflag : columns P1, P2 rotated (process_group_L); one thread per
+// row through all eight passes.
 __device__ __noinline__ void kin_cols(const ChainDesc &c, const Smem &s, double *M, int ld, int nrows,
                          int nflag) {
   const int half = c.half;
-  const int work = half * nrows;
   const double fl = (double)nflag;
-  for (int p = 0; p < 8; ++p) {
-    const int g0 = c_gorder[p] * half;
-    for (int idx = threadIdx.x; idx < work; idx += Z2_NT) {
-      int kq = idx / nrows;
-      int row = idx - kq * nrows;
-      int q = g0 + kq;
-      int p1 = s.tp[2 * q], p2 = s.tp[2 * q + 1];
-      double C = s.tc[q], S = fl * s.ts[q];
-      double a = M[row + (size_t)p1 * ld], b = M[row + (size_t)p2 * ld];
-      M[row + (size_t)p1 * ld] = a * C + b * S;
-      M[row + (size_t)p2 * ld] = a * S + b * C;
-    }
-    __syncthreads();
+  for (int row = threadIdx.x; row < nrows; row += Z2_NT) {
+    double *mr = M + row;
+    for (int p = 0; p < 8; ++p) kin_group_vec<false>(s, mr, (size_t)ld, c_gorder[p] * half, half, fl);
   }
+  __syncthreads();
 }
 
 // One group (one factor E_g) of B applied to rows / columns.
 __device__ __noinline__ void kin_group_rows(const ChainDesc &c, const Smem &s, double *M, int ld, int ncols,
                                int g, int nflag) {
-  const int half = c.half, work = half * ncols, g0 = g * half;
+  const int half = c.half, g0 = g * half;
   const double fl = (double)nflag;
-  for (int idx = threadIdx.x; idx < work; idx += Z2_NT) {
-    int kq = idx / ncols, col = idx - kq * ncols, q = g0 + kq;
-    int p1 = s.tp[2 * q], p2 = s.tp[2 * q + 1];
-    double C = s.tc[q], S = fl * s.ts[q];
-    double *mc = M + (size_t)col * ld;
-    double a = mc[p1], b = mc[p2];
-    mc[p1] = C * a + S * b;
-    mc[p2] = S * a + C * b;
-  }
+  for (int col = threadIdx.x; col < ncols; col += Z2_NT)
+    kin_group_vec<true>(s, M + (size_t)col * ld, 1, g0, half, fl);
   __syncthreads();
 }
 __device__ __noinline__ void kin_group_cols(const ChainDesc &c, const Smem &s, double *M, int ld, int nrows,
                                int g, int nflag) {
-  const int half = c.half, work = half * nrows, g0 = g * half;
+  const int half = c.half, g0 = g * half;
   const double fl = (double)nflag;
-  for (int idx = threadIdx.x; idx < work; idx += Z2_NT) {
-    int kq = idx / nrows, row = idx - kq * nrows, q = g0 + kq;
-    int p1 = s.tp[2 * q], p2 = s.tp[2 * q + 1];
-    double C = s.tc[q], S = fl * s.ts[q];
-    double a = M[row + (size_t)p1 * ld], b = M[row + (size_t)p2 * ld];
-    M[row + (size_t)p1 * ld] = a * C + b * S;
-    M[row + (size_t)p2 * ld] = a * S + b * C;
-  }
+  for (int row = threadIdx.x; row < nrows; row += Z2_NT)
+    kin_group_vec<false>(s, M + row, (size_t)ld, g0, half, fl);
   __syncthreads();
 }
 
@@ -189,99 +191,6 @@ __device__ __noinline__ void apply_pending_L(const ChainDesc &c, const Smem &s, 
 // ---------------------------------------------------------------------------
 // Stabilization (src/stabilization.f90:42-264)
 // ---------------------------------------------------------------------------
-// stab_UR (left = false) / stab_UL (left = true).  On entry A (lda) holds the
-// propagated U (UR, or UL^T); U, D, V are the chain's factors in global
-// memory (U = UR or UL^T).  W0 is an N x N global workspace.
-__device__ __noinline__ void dev_stab_U(const Smem &s, int N, double *A, int lda, double *U, double *D,
-                           double *V, double *W0, bool left) {
-  double *tau = s.vec, *vn1 = s.vec + N, *vn2 = s.vec + 2 * N, *Dn = s.vec + 3 * N;
-  int *jpvt = s.ivec;
-  blk_scale_cols(A, lda, N, N, D);                 // matUDV(:,i) *= D(i)
-  blk_geqp3(A, lda, N, jpvt, tau, vn1, vn2);       // ZGEQP3
-  blk_qdrp_scale(A, lda, N, Dn);                   // D = |R_ii|, R rows /= D
-  for (int i = threadIdx.x; i < N; i += Z2_NT) D[i] = Dn[i];
-  __syncthreads();
-  if (!left) {
-    // VR <- R * (P^T VR)     (ZLAPMR(.true.) + ZTRMM('L','U','N','N'))
-    blk_perm_rows(W0, N, V, N, N, N, jpvt, true);
-    GemmOp op{A, lda, false, true, W0, N, false, false};
-    blk_gemm(N, N, N, 1.0, op, 0.0, V, N, s.tile);
-  } else {
-    // VL <- (VL P) R^T       (ZLAPMT(.true.) + ZTRMM('R','U','C','N'))
-    blk_perm_cols(W0, N, V, N, N, N, jpvt, true);
-    GemmOp op{W0, N, false, false, A, lda, true, true};
-    blk_gemm(N, N, N, 1.0, op, 0.0, V, N, s.tile);
-  }
-  blk_org2r(A, lda, N, N, tau);                    // ZUNGQR
-  blk_copy(U, N, A, lda, N, N);                    // UR = Q, or UL^T = Q
-}
-
-// stab_green: G = (I + UR DR VR VL DL UL)^{-1} into Gout (global, ld N).
-// M (ldm) is the QR work matrix; W1, W2, W3 are N x N global workspaces.
-__device__ __noinline__ void dev_stab_green(const Smem &s, int N, int nt, int Ltrot, const double *UR,
-                               const double *DR, const double *VR, const double *ULT,
-                               const double *DL, const double *VL, double *M, int ldm,
-                               double *W1, double *W2, double *W3, double *Gout) {
-  double *tau = s.vec, *vn1 = s.vec + N, *vn2 = s.vec + 2 * N, *Dn = s.vec + 3 * N;
-  int *jpvt = s.ivec;
-  // invULUR = UR^T UL^T ; VRVL = VR VL
-  {
-    GemmOp op{UR, N, true, false, ULT, N, false, false};
-    blk_gemm(N, N, N, 1.0, op, 0.0, M, ldm, s.tile);
-    GemmOp op2{VR, N, false, false, VL, N, false, false};
-    blk_gemm(N, N, N, 1.0, op2, 0.0, W1, N, s.tile);
-  }
-  // matUDV = invULUR + DR (VRVL DL)   (src/stabilization.f90:138-146)
-  for (int j = threadIdx.x / 32; j < N; j += Z2_WARPS) {
-    double dl = DL[j];
-    for (int i = threadIdx.x & 31; i < N; i += 32) {
-      double t = W1[i + (size_t)j * N] * dl;
-      double u = DR[i] * t;
-      M[i + (size_t)j * ldm] = M[i + (size_t)j * ldm] + u;
-    }
-  }
-  __syncthreads();
-  const int half = Ltrot / 2;
-  if (nt > half) {   // matUDV = matUDV^dagger
-    for (int e = threadIdx.x; e < N * N; e += Z2_NT) {
-      int i = e % N, j = e / N;
-      if (i < j) {
-        double a = M[i + (size_t)j * ldm], b = M[j + (size_t)i * ldm];
-        M[i + (size_t)j * ldm] = b;
-        M[j + (size_t)i * ldm] = a;
-      }
-    }
-    __syncthreads();
-  }
-  blk_geqp3(M, ldm, N, jpvt, tau, vn1, vn2);
-  blk_qdrp_scale(M, ldm, N, Dn);
-  if (nt < half + 1) {
-    // G = UL^dagger P V^-1 D^-1 U^dagger UR^dagger
-    blk_transpose(W2, N, UR, N, N, N);                     // temp = UR^T
-    blk_ormqr_LT(M, ldm, N, tau, W2, N, N);                // Q^T temp
-    for (int j = threadIdx.x / 32; j < N; j += Z2_WARPS)
-      for (int i = threadIdx.x & 31; i < N; i += 32) W2[i + (size_t)j * N] = W2[i + (size_t)j * N] / Dn[i];
-    __syncthreads();
-    blk_trsm_LUN(M, ldm, N, W2, N, N);                     // V^-1 (...)
-    blk_perm_rows(W3, N, W2, N, N, N, jpvt, false);        // ZLAPMR(.false.)
-    GemmOp op{ULT, N, false, false, W3, N, false, false};  // UL^T temp
-    blk_gemm(N, N, N, 1.0, op, 0.0, Gout, N, s.tile);
-  } else {
-    // G = UL^dagger U D^-1 V P^-1 UR^dagger
-    blk_copy(W2, N, ULT, N, N, N);                         // temp = UL^T
-    blk_ormqr_RN(M, ldm, N, tau, W2, N, N);                // temp Q
-    for (int j = threadIdx.x / 32; j < N; j += Z2_WARPS) {
-      double d = Dn[j];
-      for (int i = threadIdx.x & 31; i < N; i += 32) W2[i + (size_t)j * N] = W2[i + (size_t)j * N] / d;
-    }
-    __syncthreads();
-    blk_trsm_RUT(M, ldm, N, W2, N, N);                     // (...) V^-dagger
-    blk_perm_cols(W3, N, W2, N, N, N, jpvt, false);        // ZLAPMT(.false.)
-    GemmOp op{W3, N, false, false, UR, N, true, false};    // temp UR^T
-    blk_gemm(N, N, N, 1.0, op, 0.0, Gout, N, s.tile);
-  }
-}
-
 // stab_green_big (src/stabilization.f90:202-264): the four blocks of the
 // 2N x 2N Green's function.  Inverses of the orthogonal factors (UL UR,
 // bigU, UR, UL) are their transposes; VR VL, VR and VL are inverted by LU;
@@ -386,38 +295,10 @@ __device__ __noinline__ void green_big_extract(int N, const double *B3, double *
 // ---------------------------------------------------------------------------
 // Delayed rank-2 updates (LocalK_metro, src/localK.f90:45-173)
 // ---------------------------------------------------------------------------
-// G <- G - X Yt^T over the m queued columns, 4x4 register tiles.
-__device__ __noinline__ void rank_update(double *G, int ldg, const double *X, const double *Yt, int N, int m) {
-  const int T = (N + 3) >> 2;
-  for (int t = threadIdx.x; t < T * T; t += Z2_NT) {
-    const int ti = t % T, tj = t / T;
-    double acc[4][4];
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-    int rows[4], cols[4];
-#pragma unroll
-    for (int a = 0; a < 4; ++a) { rows[a] = ti + T * a; cols[a] = 4 * tj + a; }
-    for (int q = 0; q < m; ++q) {
-      const double *xq = X + (size_t)q * N, *yq = Yt + (size_t)q * N;
-      double xa[4], yb[4];
-#pragma unroll
-      for (int a = 0; a < 4; ++a) xa[a] = rows[a] < N ? xq[rows[a]] : 0.0;
-#pragma unroll
-      for (int b = 0; b < 4; ++b) yb[b] = cols[b] < N ? yq[cols[b]] : 0.0;
-#pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = fma(xa[a], yb[b], acc[a][b]);
-    }
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int b = 0; b < 4; ++b)
-        if (rows[a] < N && cols[b] < N) G[rows[a] + (size_t)cols[b] * ldg] -= acc[a][b];
-  }
-  __syncthreads();
+// G <- G - X Yt^T over the m queued columns (ld ldx): one DMMA rank-m update.
+__device__ __forceinline__ void rank_update(double *G, int ldg, const double *X, const double *Yt,
+                                            int N, int ldx, int m) {
+  blk_dmma(N, N, m, -1.0, MatRef{X, 1, ldx}, false, MatRef{Yt, ldx, 1}, false, 1.0, G, ldg);
 }
 
 // The 2N proposals of one slice (LocalK_prop_L: bonds 2N..1, LocalK_prop_R:
@@ -425,18 +306,41 @@ __device__ __noinline__ void rank_update(double *G, int ldg, const double *X, co
 // against the current G = G0 - X Yt^T; all proposals before the first
 // accepted one are rejections (G and sigma unchanged), so they are exact.
 // One ranf draw per proposal (src/localK.f90:123), advanced in closed form.
-__device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, int nt, bool descending,
-                              int dir) {
+// The slice's sigma (and its neighbours in tau), the Delta table and the
+// plaquette partners are staged in shared memory; warp 0 keeps the ranf state
+// and the acceptance counters in registers for the whole slice.
+__device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, int nt,
+                                           bool descending, int dir) {
   const int N = c.N, nb = c.nb, k2 = c.k2, Lt = c.Ltrot;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  double *G = s.G; const int ldg = s.ldg;
+  double *G = s.G;
+  const int ldg = s.ldg;
   double *X = s.X, *Yt = s.Yt;
+  const int ldx = s.ldx;
   signed char *sg = c.sigma + (size_t)(nt - 1) * nb;
-  const signed char *sprev = c.sigma + (size_t)((nt - 2 + Lt) % Lt) * nb;
-  const signed char *snext = c.sigma + (size_t)(nt % Lt) * nb;
-  for (int i = threadIdx.x; i < nb; i += Z2_NT) s.sig[i] = sg[i];
+  const signed char *gprev = c.sigma + (size_t)((nt - 2 + Lt) % Lt) * nb;
+  const signed char *gnext = c.sigma + (size_t)(nt % Lt) * nb;
+  signed char *sig = s.sig, *sprev = s.sig + nb, *snext = s.sig + 2 * nb;
+  double *dl = s.vec;                                 // [2N][2] Delta(1,1), Delta(1,2)
+  short *bbs = reinterpret_cast<short *>(s.vec + 2 * nb);   // [2N][6]
+  for (int i = threadIdx.x; i < nb; i += Z2_NT) {
+    sig[i] = sg[i];
+    sprev[i] = gprev[i];
+    snext[i] = gnext[i];
+    dl[2 * i] = c.dlt[2 * i];
+    dl[2 * i + 1] = c.dlt[2 * i + 1];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) bbs[6 * i + q] = (short)c.bbonds[6 * i + q];
+  }
   __syncthreads();
   double *pdat = s.red + 48;      // accepted proposal: pinv(4), D11, D12
+  unsigned int st = 0;
+  long long rpos = 0;
+  int den = 0, num = 0;
+  if (warp == 0) {
+    st = *c.rng;
+    if (c.replay) rpos = *c.replay_pos;
+  }
   int m = 0, done = 0;
   while (done < nb) {
     if (warp == 0) {
@@ -447,13 +351,13 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
       double g11 = G[p1 + (size_t)p1 * ldg], g12 = G[p1 + (size_t)p2 * ldg];
       double g21 = G[p2 + (size_t)p1 * ldg], g22 = G[p2 + (size_t)p2 * ldg];
       for (int q = 0; q < m; ++q) {
-        double xa = X[p1 + (size_t)q * N], xb = X[p2 + (size_t)q * N];
-        double ya = Yt[p1 + (size_t)q * N], yb = Yt[p2 + (size_t)q * N];
+        const double xa = X[p1 + (size_t)q * ldx], xb = X[p2 + (size_t)q * ldx];
+        const double ya = Yt[p1 + (size_t)q * ldx], yb = Yt[p2 + (size_t)q * ldx];
         g11 -= xa * ya; g12 -= xa * yb; g21 -= xb * ya; g22 -= xb * yb;
       }
-      const double s_old = (double)s.sig[b];
+      const double s_old = (double)sig[b];
       const double s_new = -s_old;
-      const double D11 = c.dlt[2 * b], D12 = s_new * c.dlt[2 * b + 1];
+      const double D11 = dl[2 * b], D12 = s_new * dl[2 * b + 1];
       // (I - G)_PP, Prod = I + Delta (I - G)_PP, determinant (no FMA
       // contraction: same rounding sequence as the reference)
       const double l11 = __dsub_rn(1.0, g11), l12 = -g12, l21 = -g21, l22 = __dsub_rn(1.0, g22);
@@ -464,16 +368,13 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
       const double p11 = __dadd_rn(1.0, m11), p12 = m12, p21 = m21, p22 = __dadd_rn(1.0, m22);
       const double det = __dsub_rn(__dmul_rn(p11, p22), __dmul_rn(p12, p21));
       // boson ratio (src/fields.f90:40-119) from the host table
-      const int *bb = c.bbonds + 6 * b;
-      const double tmp_old = s_old * s.sig[bb[0]] * s.sig[bb[1]] * s.sig[bb[2]] +
-                             s_old * s.sig[bb[3]] * s.sig[bb[4]] * s.sig[bb[5]];
+      const short *bb = bbs + 6 * b;
+      const double tmp_old = s_old * sig[bb[0]] * sig[bb[1]] * sig[bb[2]] +
+                             s_old * sig[bb[3]] * sig[bb[4]] * sig[bb[5]];
       const int is = (int)(-2.0 * tmp_old + 4.0) >> 2;
       const double tn = s_old * ((double)sprev[b] + (double)snext[b]);
       const int it = (int)(-2.0 * tn + 4.0) >> 2;
       const double ratio = __dmul_rn(__dmul_rn(det, det), c.rb[is * 3 + it]);
-      // uniform: replayed or ranf
-      const unsigned int st = *c.rng;
-      long long rpos = c.replay ? *c.replay_pos : 0;
       double r;
       if (c.replay && rpos + lane < c.nreplay) r = c.replay[rpos + lane];
       else r = (double)ranf_adv(st, lane + 1) * (1.0 / 2147483648.0);
@@ -483,26 +384,23 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
       const int rem = nb - done;
       const int cnt = (first < 32) ? first + 1 : (rem < 32 ? rem : 32);
       if (lane < cnt && c.dec) {
-        size_t li = ((size_t)dir * Lt + (nt - 1)) * nb + b;
+        const size_t li = ((size_t)dir * Lt + (nt - 1)) * nb + b;
         c.dec[li] = (lane == first) ? 1 : 0;
         if (c.ratios) c.ratios[li] = ratio;
       }
       if (lane == first) {
-        const double inv = 1.0 / det;
         pdat[0] = p22 / det; pdat[1] = -p12 / det; pdat[2] = -p21 / det; pdat[3] = p11 / det;
-        (void)inv;
         pdat[4] = D11; pdat[5] = D12;
         s.flag[1] = b;
       }
+      st = ranf_adv(st, cnt);
+      rpos += cnt;
+      den += cnt;
+      num += (first < 32) ? 1 : 0;
       __syncwarp();
       if (lane == 0) {
         s.flag[0] = done + cnt;
         if (first == 32) s.flag[1] = -1;
-        *c.rng = ranf_adv(st, cnt);
-        if (c.replay) *c.replay_pos = rpos + cnt;
-        c.acc[A_ACC_DEN] += (double)cnt;
-        c.acc[A_DRAWS] += (double)cnt;
-        if (first < 32) c.acc[A_ACC_NUM] += 1.0;
       }
     }
     __syncthreads();
@@ -516,33 +414,50 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
         double u0 = G[i + (size_t)p1 * ldg], u1 = G[i + (size_t)p2 * ldg];
         double v0 = G[p1 + (size_t)i * ldg], v1 = G[p2 + (size_t)i * ldg];
         for (int q = 0; q < m; ++q) {
-          const double xi = X[i + (size_t)q * N], yi = Yt[i + (size_t)q * N];
-          u0 -= xi * Yt[p1 + (size_t)q * N];
-          u1 -= xi * Yt[p2 + (size_t)q * N];
-          v0 -= X[p1 + (size_t)q * N] * yi;
-          v1 -= X[p2 + (size_t)q * N] * yi;
+          const double xi = X[i + (size_t)q * ldx], yi = Yt[i + (size_t)q * ldx];
+          u0 -= xi * Yt[p1 + (size_t)q * ldx];
+          u1 -= xi * Yt[p2 + (size_t)q * ldx];
+          v0 -= X[p1 + (size_t)q * ldx] * yi;
+          v1 -= X[p2 + (size_t)q * ldx] * yi;
         }
         // temp = Uhlp * Prodinv ; Vhlp = Delta (I - G)(P, :)
-        X[i + (size_t)m * N] = u0 * q00 + u1 * q10;
-        X[i + (size_t)(m + 1) * N] = u0 * q01 + u1 * q11;
+        X[i + (size_t)m * ldx] = u0 * q00 + u1 * q10;
+        X[i + (size_t)(m + 1) * ldx] = u0 * q01 + u1 * q11;
         double y0 = -D11 * v0 - D12 * v1;
         double y1 = -D12 * v0 - D11 * v1;
         if (i == p1) { y0 += D11; y1 += D12; }
         if (i == p2) { y0 += D12; y1 += D11; }
-        Yt[i + (size_t)m * N] = y0;
-        Yt[i + (size_t)(m + 1) * N] = y1;
+        Yt[i + (size_t)m * ldx] = y0;
+        Yt[i + (size_t)(m + 1) * ldx] = y1;
       }
       if (threadIdx.x == 0) {
-        signed char sn = (signed char)(-s.sig[b]);
-        s.sig[b] = sn;
+        const signed char sn = (signed char)(-sig[b]);
+        sig[b] = sn;
         sg[b] = sn;
       }
       __syncthreads();
       m += 2;
-      if (m >= k2) { rank_update(G, ldg, X, Yt, N, m); m = 0; }
+      if (m >= k2) {
+        const long long tf = ph_now();
+        rank_update(G, ldg, X, Yt, N, ldx, m);
+        m = 0;
+        if (threadIdx.x == 0) c.acc[A_PH0 + PH_FLUSH] += (double)(ph_now() - tf);
+      }
     }
   }
-  if (m > 0) rank_update(G, ldg, X, Yt, N, m);
+  if (m > 0) {
+    const long long tf = ph_now();
+    rank_update(G, ldg, X, Yt, N, ldx, m);
+    if (threadIdx.x == 0) c.acc[A_PH0 + PH_FLUSH] += (double)(ph_now() - tf);
+  }
+  if (threadIdx.x == 0) {
+    *c.rng = st;
+    if (c.replay) *c.replay_pos = rpos;
+    c.acc[A_ACC_DEN] += (double)den;
+    c.acc[A_DRAWS] += (double)den;
+    c.acc[A_ACC_NUM] += (double)num;
+  }
+  __syncthreads();
 }
 
 // ---------------------------------------------------------------------------
@@ -651,6 +566,17 @@ __device__ __noinline__ void obs_tau(const ChainDesc &c, const Smem &s, int nt) 
 // ---------------------------------------------------------------------------
 struct Pend { int lo, hi; };   // lazily propagated slices, lo > hi = none
 
+// Phase timer: accumulates SM cycles of a phase into the chain's counters.
+struct PhTimer {
+  const ChainDesc &c;
+  int ph;
+  long long t0;
+  __device__ PhTimer(const ChainDesc &cc, int p) : c(cc), ph(p), t0(ph_now()) {}
+  __device__ ~PhTimer() {
+    if (threadIdx.x == 0) c.acc[A_PH0 + ph] += (double)(ph_now() - t0);
+  }
+};
+
 __device__ __forceinline__ double *qr_matrix(const ChainDesc &c, const Smem &s, int &ld) {
   ld = s.ldq;
   return s.Wq;
@@ -714,9 +640,10 @@ __device__ __noinline__ void wrap_L(const ChainDesc &c, const Smem &s, int nt, P
   }
   pd.lo = 1; pd.hi = 0;
   if (nt != c.Ltrot) {
-    dev_stab_U(s, N, A, lda, c.ULT, c.DL, c.VL, c.W0, true);
-    dev_stab_green(s, N, nt, c.Ltrot, c.UR, c.DR, c.VR, c.ULT, c.DL, c.VL, A, lda, c.W1, c.W2,
-                   c.W0, c.W3);
+    { PhTimer t(c, 6); dev_stab_U(s, N, A, lda, c.ULT, c.DL, c.VL, c.W0, true); }
+    { PhTimer t(c, 7);
+      dev_stab_green(s, N, nt, c.Ltrot, c.UR, c.DR, c.VR, c.ULT, c.DL, c.VL, A, lda, c.W1, c.W2,
+                     c.W0, c.W3); }
     double dif = blk_maxdiff(c.W3, N, c.G, N, N, s.red);
     record_drift(c, dif, stats);
     blk_copy(c.G, N, c.W3, N, N, N);
@@ -745,9 +672,10 @@ __device__ __noinline__ void wrap_R(const ChainDesc &c, const Smem &s, int nt, P
   }
   pd.lo = 1; pd.hi = 0;
   if (nt != 0) {
-    dev_stab_U(s, N, A, lda, c.UR, c.DR, c.VR, c.W0, false);
-    dev_stab_green(s, N, nt, c.Ltrot, c.UR, c.DR, c.VR, c.ULT, c.DL, c.VL, A, lda, c.W1, c.W2,
-                   c.W0, c.W3);
+    { PhTimer t(c, 6); dev_stab_U(s, N, A, lda, c.UR, c.DR, c.VR, c.W0, false); }
+    { PhTimer t(c, 7);
+      dev_stab_green(s, N, nt, c.Ltrot, c.UR, c.DR, c.VR, c.ULT, c.DL, c.VL, A, lda, c.W1, c.W2,
+                     c.W0, c.W3); }
     double dif = blk_maxdiff(c.W3, N, c.G, N, N, s.red);
     record_drift(c, dif, stats);
     blk_copy(c.G, N, c.W3, N, N, N);

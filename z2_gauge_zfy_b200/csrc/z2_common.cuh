@@ -23,8 +23,15 @@ enum {
   A_TXMAX0, A_TXMAX1, A_TXMAX2, A_TXMEAN0, A_TXMEAN1, A_TXMEAN2,
   A_BIN0,                        // 7 bin results: flux_avg .. density
   A_LOGDET = A_BIN0 + 7, A_DMU, A_DRAWS,
-  A_COUNT
+  A_PH0,                         // Z2_NPHASE per-phase SM cycle counters
+  A_COUNT = A_PH0 + 8
 };
+
+// Phases of a bin timed with clock64() by thread 0 (tracing; no effect on
+// results): checkerboard wrap of G, proposals (evaluation + rank-2 bookkeeping),
+// rank-2k flushes, equal-time observables, wraps/stabilization, the
+// time-displaced chain.
+enum { PH_KIN = 0, PH_PROP, PH_FLUSH, PH_OBS, PH_WRAP, PH_DYN, PH_COUNT = 8 };
 
 // Status flags (ChainDesc::status).
 enum { ST_NONFINITE = 1, ST_BADARG = 2 };
@@ -91,7 +98,8 @@ struct Smem {
   double *arena;    // big region
   double *G;        // G (smem arena or global)
   int ldg;          // leading dimension of G
-  double *X, *Yt;   // delayed-update factors [N][k2]
+  double *X, *Yt;   // delayed-update factors [k2][ldx]
+  int ldx;          // odd leading dimension of X, Yt
   double *Wq;       // QR work matrix (arena or global)
   int ldq;
   double *tile;     // GEMM/panel staging (arena tail)
@@ -150,6 +158,8 @@ __device__ __forceinline__ void blk_sum_n(double *v, double *red) {
     v[q] = t;
   }
 }
+
+__device__ __forceinline__ long long ph_now() { return clock64(); }
 
 // ranf multiplier powers IP^i mod 2^31, i = 0..32 (filled by the host).
 __constant__ unsigned int c_ipow[33];

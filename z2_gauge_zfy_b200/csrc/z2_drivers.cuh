@@ -98,38 +98,44 @@ __device__ __noinline__ void sweep_L(const ChainDesc &c, const Smem &s) {
   const int N = c.N;
   Pend pd{1, 0};
   for (int nt = c.Ltrot; nt >= 1; --nt) {
-    if (nt % c.Nwrap == 0) wrap_L(c, s, nt, pd, true);
-    obs_equal(c, s, nt);
+    if (nt % c.Nwrap == 0) { PhTimer t(c, PH_WRAP); wrap_L(c, s, nt, pd, true); }
+    { PhTimer t(c, PH_OBS); obs_equal(c, s, nt); }
     scale_G_mu(c, s);                               // propT_L
-    propose_slice(c, s, nt, true, 0);               // LocalK_prop_L: bonds 2N..1
-    build_table(c, s, nt);
-    kin_cols(c, s, s.G, s.ldg, N, 1);               // G B
-    kin_rows(c, s, s.G, s.ldg, N, -1);              // B^-1 G
+    { PhTimer t(c, PH_PROP); propose_slice(c, s, nt, true, 0); }   // bonds 2N..1
+    {
+      PhTimer t(c, PH_KIN);
+      build_table(c, s, nt);
+      kin_cols(c, s, s.G, s.ldg, N, 1);             // G B
+      kin_rows(c, s, s.G, s.ldg, N, -1);            // B^-1 G
+    }
     if (pd.lo > pd.hi) { pd.lo = nt; pd.hi = nt; } else pd.lo = nt;
   }
-  wrap_L(c, s, 0, pd, true);
+  { PhTimer t(c, PH_WRAP); wrap_L(c, s, 0, pd, true); }
 }
 
 // Local_sweep_R (src/local_sweep.f90:126-150)
 __device__ __noinline__ void sweep_R(const ChainDesc &c, const Smem &s, bool toggle) {
   const int N = c.N;
   if (toggle) {
-    dyn_sweep(c, s);
+    { PhTimer t(c, PH_DYN); dyn_sweep(c, s); }
     if (threadIdx.x == 0) c.acc[A_NOBST] += 1.0;
     __syncthreads();
     load_G(c, s);     // the time-displaced pass used the arena
   }
   Pend pd{1, 0};
-  wrap_R(c, s, 0, pd, true);
+  { PhTimer t(c, PH_WRAP); wrap_R(c, s, 0, pd, true); }
   for (int nt = 1; nt <= c.Ltrot; ++nt) {
-    build_table(c, s, nt);
-    kin_rows(c, s, s.G, s.ldg, N, 1);               // B G
-    kin_cols(c, s, s.G, s.ldg, N, -1);              // G B^-1
-    propose_slice(c, s, nt, false, 1);              // LocalK_prop_R: bonds 1..2N
+    {
+      PhTimer t(c, PH_KIN);
+      build_table(c, s, nt);
+      kin_rows(c, s, s.G, s.ldg, N, 1);             // B G
+      kin_cols(c, s, s.G, s.ldg, N, -1);            // G B^-1
+    }
+    { PhTimer t(c, PH_PROP); propose_slice(c, s, nt, false, 1); }  // bonds 1..2N
     if (pd.lo > pd.hi) { pd.lo = nt; pd.hi = nt; } else pd.hi = nt;
     scale_G_mu(c, s);                               // propT_R
-    if (nt % c.Nwrap == 0) wrap_R(c, s, nt, pd, true);
-    obs_equal(c, s, nt);
+    if (nt % c.Nwrap == 0) { PhTimer t(c, PH_WRAP); wrap_R(c, s, nt, pd, true); }
+    { PhTimer t(c, PH_OBS); obs_equal(c, s, nt); }
   }
 }
 

@@ -19,9 +19,20 @@ __device__ __forceinline__ double dlapy2(double x, double y) {
   return w * sqrt(1.0 + q * q);
 }
 
+// Element copies are issued in batches of 4 loads before 4 stores (dst and
+// src may be the same allocation, so the compiler keeps program order).
 __device__ __noinline__ void blk_copy(double *dst, int ldd, const double *src, int lds, int m, int n) {
-  for (int j = threadIdx.x / 32; j < n; j += Z2_WARPS)
-    for (int i = threadIdx.x & 31; i < m; i += 32) dst[i + (size_t)j * ldd] = src[i + (size_t)j * lds];
+  const int lane = threadIdx.x & 31;
+  for (int j = threadIdx.x / 32; j < n; j += Z2_WARPS) {
+    const double *s = src + (size_t)j * lds;
+    double *d = dst + (size_t)j * ldd;
+    int i = lane;
+    for (; i + 96 < m; i += 128) {
+      const double a0 = s[i], a1 = s[i + 32], a2 = s[i + 64], a3 = s[i + 96];
+      d[i] = a0; d[i + 32] = a1; d[i + 64] = a2; d[i + 96] = a3;
+    }
+    for (; i < m; i += 32) d[i] = s[i];
+  }
   __syncthreads();
 }
 // dst = src^T (src m x n -> dst n x m)
