@@ -71,6 +71,8 @@ typedef struct z2_options {
   int32_t record;    /* 1: keep decisions and ratios of each half-sweep */
   int32_t device;    /* CUDA device ordinal */
   int32_t tau;       /* 1: allocate the time-displaced chain (is_tau) */
+  int32_t graph;     /* 1: capture each bin's launch as a CUDA graph, replayed */
+  const int32_t *delay_k_chain;  /* optional [nchains] per-chain delay rank (autotuner) */
 } z2_options;
 
 typedef struct z2_handle z2_handle;

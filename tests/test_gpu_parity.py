@@ -239,3 +239,35 @@ def test_logdet_grad_parity():
     assert abs(ld - ld_o) <= 1e-10 * abs(ld_o)
     assert rel(g, g_o) < 1e-9
     assert abs(dmu - dmu_o) <= 1e-10 * abs(dmu_o)
+
+
+def test_sweep_parity_L16_global_G():
+    """N = 256: G does not fit in shared memory and lives in global memory
+    (same kernels through generic pointers)."""
+    ch = Chain(RT=1.0, J=0.5, h=0.6, mu=0.0, Nlx=16, Nly=16, Ltrot=16, beta=0.8, Nwrap=8,
+               seed=4321)
+    c, res = _run_pair(ch)
+    G, obs, st, (dec, rat), _, (sig, iseed) = res[-1]
+    dec_o, _ = _decisions_oracle(c, ch.Ltrot, 2 * ch.N)
+    assert np.array_equal(dec, dec_o)
+    assert np.array_equal(sig, c.sigma) and iseed == c.rng.state
+    assert rel(G, c.prop.Gr) < RTOL
+
+
+def test_graph_replay_and_delay_rank_identical_decisions():
+    chains = [Chain(RT=1.0, J=0.5, h=0.5, Nlx=6, Nly=6, Ltrot=20, beta=2.0, Nwrap=10, seed=s)
+              for s in (11, 12)]
+    outs = []
+    for kw in (dict(), dict(graph=True), dict(delay_k_chain=[4, 32])):
+        with Z2Batch(chains, record=True, **kw) as b:
+            b.pre()
+            for _ in range(3):
+                b.sweep(1, False)
+            outs.append([(b.green(i), b.decisions(i)[0], b.get_config(i)[0]) for i in range(2)])
+    for i in range(2):
+        g0, d0, s0 = outs[0][i]
+        g1, d1, s1 = outs[1][i]
+        assert np.array_equal(g0, g1) and np.array_equal(d0, d1) and np.array_equal(s0, s1)
+        g2, d2, s2 = outs[2][i]
+        assert np.array_equal(d0, d2) and np.array_equal(s0, s2)
+        assert rel(g2, g0) < RTOL

@@ -65,7 +65,7 @@ class Z2Batch:
     """A batch of chains resident on one GPU (``z2_create``)."""
 
     def __init__(self, chains, delay_k: int = 0, record: bool = False, device: int = 0,
-                 tau: bool = False):
+                 tau: bool = False, graph: bool = False, delay_k_chain=None):
         self.lib = _ffi.load()
         self.chains = list(chains)
         n = len(self.chains)
@@ -83,7 +83,14 @@ class Z2Batch:
                 p.rt_bond = dptr(rb)
             else:
                 p.rt_bond = None
-        opt = Options(delay_k, 1 if record else 0, device, 1 if tau else 0)
+        self._kc = None
+        kc_ptr = None
+        if delay_k_chain is not None:
+            self._kc = np.ascontiguousarray(delay_k_chain, dtype=np.int32)
+            assert self._kc.shape == (n,)
+            kc_ptr = self._kc.ctypes.data_as(C.POINTER(C.c_int32))
+        opt = Options(delay_k, 1 if record else 0, device, 1 if tau else 0, 1 if graph else 0,
+                      kc_ptr)
         h = C.c_void_p()
         code = self.lib.z2_create(C.byref(h), arr, n, C.byref(opt))
         self.h = h

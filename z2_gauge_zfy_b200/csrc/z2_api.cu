@@ -211,6 +211,12 @@ struct z2_handle {
   bool pre_done = false;
   // unit-op scratch
   double *u_buf = nullptr;
+  // per-chain status flags in one array (one readback per launch)
+  int *d_status = nullptr;
+  std::vector<int> h_status;
+  // CUDA graphs of the bin launch, keyed by (nsweep, toggle)
+  struct GraphEntry { int nsweep, toggle; cudaGraphExec_t exec; };
+  std::vector<GraphEntry> graphs;
   size_t u_n = 0;
 };
 
@@ -293,6 +299,20 @@ extern "C" int z2_create(z2_handle **out, const z2_chain_params *params, int32_t
   h->nchains = nchains;
   if (opt) h->opt = *opt;
   h->device = h->opt.device;
+  // argument checks first (the reference stops on these, src/calc_basic.f90:96-100,
+  // src/fields.f90:422-424), before any CUDA call
+  for (int c = 0; c < nchains; ++c) {
+    const z2_chain_params &p = params[c];
+    if (p.Nlx < 2 || p.Nly < 2 || (p.Nlx % 2) || (p.Nly % 2))
+      return set_err(h, Z2_ERR_ARG, "chain %d: Nlx, Nly must be even and >= 2", c);
+    if (p.Ltrot < 1 || p.Nwrap < 1 || p.Ltrot % p.Nwrap)
+      return set_err(h, Z2_ERR_ARG, "chain %d: Ltrot must be a multiple of Nwrap", c);
+    if (p.absolute < 1 || p.absolute > 5)
+      return set_err(h, Z2_ERR_ARG, "chain %d: incorrect absolute input %d", c, p.absolute);
+    if (!(p.beta > 0.0)) return set_err(h, Z2_ERR_ARG, "chain %d: beta must be positive", c);
+    if (p.Nlx * p.Nly > 1024)
+      return set_err(h, Z2_ERR_ARG, "chain %d: N = %d exceeds 1024", c, p.Nlx * p.Nly);
+  }
   CUDA_TRY(h, cudaSetDevice(h->device));
   // ranf multiplier powers
   {
@@ -327,6 +347,8 @@ extern "C" int z2_create(z2_handle **out, const z2_chain_params *params, int32_t
     const int ldg = (N % 2) ? N : N + 1;
     int small = smem_small_bytes(N);
     int k = h->opt.delay_k > 0 ? h->opt.delay_k : default_k(N);
+    if (h->opt.delay_k_chain && h->opt.delay_k_chain[c] > 0) k = h->opt.delay_k_chain[c];
+    if (k > 64) k = 64;
     size_t arena = (size_t)(kSmemMax - small) / 8;
     size_t nn = (size_t)N * ldg;
     int g_in = 0;
@@ -363,6 +385,9 @@ extern "C" int z2_create(z2_handle **out, const z2_chain_params *params, int32_t
                                    (int)h->smem));
   CUDA_TRY(h, cudaFuncSetAttribute(z2_unit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)h->smem));
+  CUDA_TRY(h, cudaMalloc(&h->d_status, sizeof(int) * nchains));
+  CUDA_TRY(h, cudaMemset(h->d_status, 0, sizeof(int) * nchains));
+  h->h_status.assign(nchains, 0);
   // device memory and tables
   for (int c = 0; c < nchains; ++c) {
     ChainHost &C = h->ch[c];
@@ -493,7 +518,7 @@ extern "C" int z2_create(z2_handle **out, const z2_chain_params *params, int32_t
     char *misc = base + o_misc;
     d.rng = (unsigned int *)misc;
     d.replay_pos = (long long *)(misc + 8);
-    d.status = (int *)(misc + 16);
+    d.status = h->d_status + c;
     d.replay = nullptr; d.nreplay = 0;
     d.dec = h->opt.record ? (unsigned char *)(base + o_dec) : nullptr;
     d.ratios = h->opt.record ? (double *)(base + o_rat) : nullptr;
@@ -540,6 +565,8 @@ extern "C" int z2_destroy(z2_handle *h) {
   if (h->d_order) cudaFree(h->d_order);
   if (h->d_queue) cudaFree(h->d_queue);
   if (h->u_buf) cudaFree(h->u_buf);
+  if (h->d_status) cudaFree(h->d_status);
+  for (auto &g : h->graphs) cudaGraphExecDestroy(g.exec);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -602,23 +629,50 @@ extern "C" int z2_get_config(const z2_handle *h, int32_t chain, double *sigma, i
   return Z2_OK;
 }
 
-static int launch_chains(z2_handle *h, int op, int nsweep, int toggle, float *ms) {
-  CUDA_TRY(h, cudaSetDevice(h->device));
+static int enqueue_chains(z2_handle *h, int op, int nsweep, int toggle) {
   CUDA_TRY(h, cudaMemsetAsync(h->d_queue, 0, sizeof(int), h->stream));
-  if (ms) CUDA_TRY(h, cudaEventRecord(h->ev0, h->stream));
   z2_chain_kernel<<<h->grid, Z2_NT, h->smem, h->stream>>>(h->d_desc, h->d_order, h->nchains,
                                                           h->d_queue, op, nsweep, toggle, h->smem);
   CUDA_TRY(h, cudaGetLastError());
+  return Z2_OK;
+}
+
+static int launch_chains(z2_handle *h, int op, int nsweep, int toggle, float *ms) {
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  cudaGraphExec_t exec = nullptr;
+  if (h->opt.graph && op == OP_SWEEP) {
+    for (auto &g : h->graphs)
+      if (g.nsweep == nsweep && g.toggle == toggle) exec = g.exec;
+    if (!exec) {
+      // capture the bin (queue reset + persistent launch) once, replay after
+      cudaGraph_t graph = nullptr;
+      CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+      int r = enqueue_chains(h, op, nsweep, toggle);
+      cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+      if (r) return r;
+      if (e != cudaSuccess) return set_err(h, Z2_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+      e = cudaGraphInstantiate(&exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) return set_err(h, Z2_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+      h->graphs.push_back({nsweep, toggle, exec});
+    }
+  }
+  if (ms) CUDA_TRY(h, cudaEventRecord(h->ev0, h->stream));
+  if (exec) {
+    CUDA_TRY(h, cudaGraphLaunch(exec, h->stream));
+  } else {
+    int r = enqueue_chains(h, op, nsweep, toggle);
+    if (r) return r;
+  }
   if (ms) CUDA_TRY(h, cudaEventRecord(h->ev1, h->stream));
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   if (ms) CUDA_TRY(h, cudaEventElapsedTime(ms, h->ev0, h->ev1));
-  // status flags
-  for (int c = 0; c < h->nchains; ++c) {
-    int st = 0;
-    CUDA_TRY(h, cudaMemcpy(&st, h->ch[c].d.status, 4, cudaMemcpyDeviceToHost));
-    if (st & ST_NONFINITE)
+  // status flags of every chain, one readback
+  CUDA_TRY(h, cudaMemcpy(h->h_status.data(), h->d_status, sizeof(int) * h->nchains,
+                         cudaMemcpyDeviceToHost));
+  for (int c = 0; c < h->nchains; ++c)
+    if (h->h_status[c] & ST_NONFINITE)
       return set_err(h, Z2_ERR_NONFINITE, "chain %d: non-finite Green's function", c);
-  }
   return Z2_OK;
 }
 
