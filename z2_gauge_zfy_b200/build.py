@@ -39,15 +39,33 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(s) <= t for s in sources())
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and up_to_date():
-        return OUT
-    cmd = [nvcc(), *NVCC_FLAGS, "-o", OUT + ".tmp", SRC]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-        print(" ".join(cmd), flush=True)
+DRIVER_SRC = os.path.join(HERE, "csrc", "z2_main.cpp")
+DRIVER = os.path.join(HERE, "z2_gauge_b200")
+
+
+def build_driver(force: bool = False) -> str:
+    """The host driver (restates src/main.f90 over the C ABI), linked to the
+    in-tree library with an $ORIGIN rpath."""
+    if (not force and os.path.exists(DRIVER)
+            and os.path.getmtime(DRIVER) >= max(os.path.getmtime(DRIVER_SRC),
+                                                os.path.getmtime(OUT))):
+        return DRIVER
+    cmd = ["g++", "-O2", "-std=c++17", DRIVER_SRC, "-L" + HERE, "-lz2dqmc",
+           "-Wl,-rpath,$ORIGIN", "-o", DRIVER + ".tmp"]
     subprocess.run(cmd, check=True)
-    os.replace(OUT + ".tmp", OUT)
+    os.replace(DRIVER + ".tmp", DRIVER)
+    return DRIVER
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if force or not up_to_date():
+        cmd = [nvcc(), *NVCC_FLAGS, "-o", OUT + ".tmp", SRC]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+        os.replace(OUT + ".tmp", OUT)
+    build_driver(force)
     return OUT
 
 

@@ -1,0 +1,344 @@
+// z2_main.cpp -- host driver over the C ABI, restating the flow of the
+// reference program (src/main.f90) for the local-sweep path:
+//
+//   paramC_sets.txt  (read_input, src/calc_basic.f90:50-89)
+//   confin.txt / seeds.txt -> sigma (conf_therm_in + conf_set + conf_transfer,
+//                                    src/fields.f90:214-507)
+//   optional boson-only warm-up (LocalK_therm, src/localK.f90:400-420)
+//   Sweep_local%pre, then Nbin bins of Sweep_local%sweep (src/main.f90:72-103)
+//   per bin: flux_avg, chi_flux, pair_sc_q0, cdw_pi, cdw_ratio, density
+//            appended, averaged over chains (Fourier%preq, src/fourier_trans.f90:251-315)
+//   info.txt summary and confout.txt (src/main.f90:104-134, src/fields.f90:509-557)
+//
+// One chain per "rank": --chains N runs N independent chains in one batch on
+// one GPU (the reference runs one per MPI rank; seeds.txt gives one seed per
+// chain).  Global moves (is_global) are not part of this path and are refused.
+//
+//   z2_gauge_b200 [--chains N] [--device D] [--dir PATH]
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/z2dqmc.h"
+
+namespace {
+
+struct Params {
+  double RT = 1, J = 0.5, h = 0.5, mu = 0, Q = 1;
+  int Nlx = 4, Nly = 4, Ltrot = 40;
+  double beta = 4;
+  int NlxT = 4, NlyT = 4, LtrotT = 40;
+  int Nwrap = 10, Nbin = 1, Nsweep = 1;
+  bool is_tau = false; int Nthermal = 0;
+  bool is_warm = false; int Nwarm = 0;
+  bool is_global = false; int Nglobal = 0;
+  int absolute = 1;
+};
+
+bool logical(const std::string &t) {
+  std::string s;
+  for (char c : t) if (c != '.') s += (char)std::tolower(c);
+  return s == "true" || s == "t";
+}
+
+bool read_params(const std::string &path, Params &p) {
+  std::ifstream f(path);
+  if (!f) return false;
+  std::vector<std::vector<std::string>> lines;
+  std::string ln;
+  while (lines.size() < 8 && std::getline(f, ln)) {
+    std::istringstream is(ln);
+    std::vector<std::string> tok;
+    std::string t;
+    while (is >> t) tok.push_back(t);
+    if (!tok.empty()) lines.push_back(tok);
+  }
+  if (lines.size() < 8) return false;
+  auto D = [&](int l, int k) { return std::atof(lines[l].at(k).c_str()); };
+  auto I = [&](int l, int k) { return std::atoi(lines[l].at(k).c_str()); };
+  p.RT = D(0, 0); p.J = D(0, 1); p.h = D(0, 2); p.mu = D(0, 3); p.Q = D(0, 4);
+  p.Nlx = I(1, 0); p.Nly = I(1, 1); p.Ltrot = I(1, 2); p.beta = D(1, 3);
+  p.NlxT = I(2, 0); p.NlyT = I(2, 1); p.LtrotT = I(2, 2);
+  p.Nwrap = I(3, 0); p.Nbin = I(3, 1); p.Nsweep = I(3, 2);
+  p.is_tau = logical(lines[4][0]); p.Nthermal = I(4, 1);
+  p.is_warm = logical(lines[5][0]); p.Nwarm = I(5, 1);
+  p.is_global = logical(lines[6][0]); p.Nglobal = I(6, 1);
+  p.absolute = I(7, 0);
+  return true;
+}
+
+// ranf (lib/package_of_matrix/Ran/ran_imada.f:55-68)
+double ranf(uint32_t &iq) {
+  iq = (uint32_t)(((uint64_t)iq * 48828125ull) & 0x7fffffffull);
+  return (double)iq / 2147483648.0;
+}
+
+int npbc(int nr, int L) { return nr < 1 ? nr + L : (nr > L ? nr - L : nr); }
+
+// conf_set on the thermalisation lattice (src/fields.f90:311-427);
+// sigma[(nt) * 2*LqT + b], lambda is drawn (and discarded: not on this path).
+void conf_set(const Params &p, std::vector<double> &s, uint32_t &iq) {
+  const int nb = 2 * p.NlxT * p.NlyT, lt = p.LtrotT;
+  s.assign((size_t)nb * lt, 1.0);
+  if (p.absolute == 1) {
+    for (int nt = 0; nt < lt; ++nt)
+      for (int b = 0; b < nb; ++b) s[(size_t)nt * nb + b] = ranf(iq) >= 0.5 ? 1.0 : -1.0;
+  } else if (p.absolute == 2) {
+    for (int nt = 0; nt < lt; ++nt)
+      for (int b = 0; b < nb; ++b) {
+        double x1 = ranf(iq), x2 = ranf(iq);
+        double x = std::sqrt(-2.0 * std::log(x1)) * std::cos(2.0 * M_PI * x2);
+        s[(size_t)nt * nb + b] = x >= 0.0 ? 1.0 : -1.0;
+      }
+  } else if (p.absolute == 4) {
+    for (int nt = 0; nt < lt; ++nt)
+      for (int b = 0; b < nb; ++b) {
+        int site = b / 2, nx = site % p.NlxT + 1, ny = site / p.NlxT + 1;
+        s[(size_t)nt * nb + b] = ((nx + ny) % 2 == 0) ? 1.0 : -1.0;
+      }
+  } else if (p.absolute == 5) {
+    for (int b = 0; b < nb; ++b) {
+      double v = ranf(iq) >= 0.5 ? 1.0 : -1.0;
+      for (int nt = 0; nt < lt; ++nt) s[(size_t)nt * nb + b] = v;
+    }
+  }
+  for (int i = 0; i < p.NlxT * p.NlyT; ++i) ranf(iq);   // lambda_random_fill
+}
+
+// conf_transfer (src/fields.f90:429-507): tile the thermalisation lattice and
+// time extent up to the run size.
+std::vector<double> conf_transfer(const Params &p, const std::vector<double> &st) {
+  const int nb = 2 * p.Nlx * p.Nly, nbT = 2 * p.NlxT * p.NlyT;
+  std::vector<double> s((size_t)nb * p.Ltrot, 1.0);
+  for (int nt = 0; nt < std::min(p.LtrotT, p.Ltrot); ++nt)
+    for (int b = 0; b < nb; ++b) {
+      int site = b / 2, nx = site % p.Nlx + 1, ny = site / p.Nlx + 1;
+      int nxt = (nx - 1) % p.NlxT + 1, nyt = (ny - 1) % p.NlyT + 1;
+      int bt = (nyt - 1) * p.NlxT * 2 + (nxt - 1) * 2 + (b % 2);   // +x: 1, +y: 2 (0-based)
+      s[(size_t)nt * nb + b] = st[(size_t)nt * nbT + bt];
+    }
+  for (int nt = p.LtrotT; nt < p.Ltrot; ++nt)
+    for (int b = 0; b < nb; ++b) s[(size_t)nt * nb + b] = s[(size_t)(nt - p.LtrotT) * nb + b];
+  return s;
+}
+
+// LocalK_therm sweep on the host (src/localK.f90:400-420, src/local_sweep.f90:73-85).
+struct Warm {
+  int Lx, Ly, N, nb, Lt;
+  std::vector<int> bb;   // [nb][6] plaquette partners (src/lattice.f90:104-141)
+  double rb[9];
+  explicit Warm(const Params &p) : Lx(p.Nlx), Ly(p.Nly), N(p.Nlx * p.Nly), nb(2 * N), Lt(p.Ltrot) {
+    auto site = [&](int x, int y) { return (y - 1) * Lx + (x - 1); };
+    auto bond = [&](int a, int b2) -> int {   // inv_bond_list
+      int ax = a % Lx + 1, ay = a / Lx + 1;
+      if (site(npbc(ax + 1, Lx), ay) == b2) return 2 * a;
+      return 2 * a + 1;
+    };
+    bb.assign(6 * nb, 0);
+    for (int nc = 0; nc < nb; ++nc) {
+      int ii = nc / 2, ix = ii % Lx + 1, iy = ii / Lx + 1;
+      int *o = &bb[6 * nc];
+      if (nc % 2 == 0) {
+        int jj = site(npbc(ix + 1, Lx), iy), jx = jj % Lx + 1, jy = jj / Lx + 1;
+        int nx = site(ix, npbc(iy + 1, Ly)); o[0] = bond(ii, nx);
+        int ny = site(jx, npbc(jy + 1, Ly)); o[1] = bond(nx, ny); o[2] = bond(jj, ny);
+        nx = site(ix, npbc(iy - 1, Ly)); o[3] = bond(nx, ii);
+        ny = site(jx, npbc(jy - 1, Ly)); o[4] = bond(nx, ny); o[5] = bond(ny, jj);
+      } else {
+        int jj = site(ix, npbc(iy + 1, Ly)), jx = jj % Lx + 1, jy = jj / Lx + 1;
+        int nx = site(npbc(jx - 1, Lx), jy); o[0] = bond(nx, jj);
+        int ny = site(npbc(ix - 1, Lx), iy); o[1] = bond(ny, nx); o[2] = bond(ny, ii);
+        nx = site(npbc(jx + 1, Lx), jy); o[3] = bond(jj, nx);
+        ny = site(npbc(ix + 1, Lx), iy); o[4] = bond(ny, nx); o[5] = bond(ii, ny);
+      }
+    }
+    const double dtau = p.beta / p.Ltrot, alpha = dtau * p.J, lub = std::log(1.0e200);
+    double gamma = 0.0; bool temporal = false;
+    if (std::fabs(p.h) > 1.0e-10) {
+      double ta = std::tanh(dtau * p.h);
+      if (ta < 1.0e-300) ta = 1.0e-300;
+      gamma = -0.5 * std::log(ta); temporal = true;
+    }
+    for (int is = 0; is < 3; ++is)
+      for (int it = 0; it < 3; ++it) {
+        double e = std::min(std::max(alpha * (4.0 * is - 4.0), -lub), lub), r = std::exp(e);
+        if (temporal) r = r * std::exp(std::min(std::max(gamma * (4.0 * it - 4.0), -lub), lub));
+        rb[is * 3 + it] = r;
+      }
+  }
+  // one therm sweep; returns accepted count
+  int sweep(std::vector<double> &s, uint32_t &iq) const {
+    int acc = 0;
+    for (int nt = 0; nt < Lt; ++nt) {
+      double *sg = &s[(size_t)nt * nb];
+      const double *sp = &s[(size_t)((nt - 1 + Lt) % Lt) * nb], *sn = &s[(size_t)((nt + 1) % Lt) * nb];
+      for (int b = 0; b < nb; ++b) {
+        const int *o = &bb[6 * b];
+        double so = sg[b];
+        double to = so * sg[o[0]] * sg[o[1]] * sg[o[2]] + so * sg[o[3]] * sg[o[4]] * sg[o[5]];
+        int is = (int)(-2.0 * to + 4.0) >> 2;
+        int it = (int)(-2.0 * so * (sp[b] + sn[b]) + 4.0) >> 2;
+        if (rb[is * 3 + it] > ranf(iq)) { sg[b] = -so; ++acc; }
+      }
+    }
+    return acc;
+  }
+};
+
+void append(const std::string &dir, const char *name, double v) {
+  FILE *f = std::fopen((dir + "/" + name).c_str(), "a");
+  if (!f) return;
+  std::fprintf(f, " %25.17E\n", v);
+  std::fclose(f);
+}
+
+int fail(z2_handle *h, const char *what, int code) {
+  std::fprintf(stderr, "%s failed (%d): %s\n", what, code, h ? z2_last_error(h) : "");
+  return 1;
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+  int nch = 1, device = 0;
+  std::string dir = ".";
+  for (int i = 1; i < argc; ++i) {
+    if (!std::strcmp(argv[i], "--chains") && i + 1 < argc) nch = std::atoi(argv[++i]);
+    else if (!std::strcmp(argv[i], "--device") && i + 1 < argc) device = std::atoi(argv[++i]);
+    else if (!std::strcmp(argv[i], "--dir") && i + 1 < argc) dir = argv[++i];
+  }
+  auto t0 = std::chrono::steady_clock::now();
+  Params p;
+  if (!read_params(dir + "/paramC_sets.txt", p)) {
+    std::fprintf(stderr, "cannot read %s/paramC_sets.txt\n", dir.c_str());
+    return 1;
+  }
+  if (p.is_global) {
+    std::fprintf(stderr, "is_global: global moves are not part of this path\n");
+    return 1;
+  }
+  if (p.Ltrot % p.Nwrap) { std::fprintf(stderr, "Ltrot must be a multiple of Nwrap\n"); return 1; }
+  const int N = p.Nlx * p.Nly, nb = 2 * N;
+  // initial configurations (conf_therm_in, src/fields.f90:227-309)
+  std::vector<std::vector<double>> sig(nch);
+  std::vector<uint32_t> iseed(nch, 0);
+  {
+    std::ifstream cin_(dir + "/confin.txt");
+    long long first = 0;
+    if (!(cin_ >> first)) first = 0;
+    if (first == 0) {
+      std::ifstream sf(dir + "/seeds.txt");
+      for (int c = 0; c < nch; ++c) {
+        long long s = 0;
+        if (!(sf >> s)) { std::fprintf(stderr, "seeds.txt has fewer than %d seeds\n", nch); return 1; }
+        uint32_t iq = (uint32_t)(int32_t)s;
+        std::vector<double> st;
+        conf_set(p, st, iq);
+        sig[c] = conf_transfer(p, st);
+        iseed[c] = iq;
+      }
+    } else {
+      // rank blocks: iseed, sigma(2*LqT, LtrotT), lambda(LqT)
+      const int nbT = 2 * p.NlxT * p.NlyT;
+      for (int c = 0; c < nch; ++c) {
+        long long s = (c == 0) ? first : 0;
+        if (c > 0 && !(cin_ >> s)) { std::fprintf(stderr, "confin.txt: missing rank %d\n", c); return 1; }
+        std::vector<double> st((size_t)nbT * p.LtrotT);
+        for (auto &x : st) if (!(cin_ >> x)) { std::fprintf(stderr, "confin.txt truncated\n"); return 1; }
+        for (int i = 0; i < p.NlxT * p.NlyT; ++i) { double l; cin_ >> l; }
+        sig[c] = conf_transfer(p, st);
+        iseed[c] = (uint32_t)(int32_t)s;
+      }
+    }
+  }
+  FILE *info = std::fopen((dir + "/info.txt").c_str(), "w");
+  if (info) {
+    std::fprintf(info, " ==============================================\n");
+    std::fprintf(info, " Lx %d Ly %d RT %.17g J %.17g h %.17g mu %.17g Q %.17g absolute %d\n", p.Nlx,
+                 p.Nly, p.RT, p.J, p.h, p.mu, p.Q, p.absolute);
+    std::fprintf(info, " Beta %.17g Ltrot %d Dtau %.17g Nwrap %d Nbin %d Nsweep %d chains %d\n",
+                 p.beta, p.Ltrot, p.beta / p.Ltrot, p.Nwrap, p.Nbin, p.Nsweep, nch);
+    std::fprintf(info, " ==============================================\n");
+  }
+  // boson warm-up on the host
+  if (p.is_warm && p.Nwarm > 0) {
+    Warm w(p);
+    double acc = 0.0;
+    for (int c = 0; c < nch; ++c)
+      for (int n = 0; n < p.Nwarm; ++n) acc += w.sweep(sig[c], iseed[c]) / double(nb * p.Ltrot);
+    if (info) std::fprintf(info, " Thermalize Accept Ratio : %.17g\n", acc / (nch * p.Nwarm));
+  }
+  std::vector<z2_chain_params> cp(nch);
+  for (int c = 0; c < nch; ++c)
+    cp[c] = z2_chain_params{p.RT, p.J, p.h, p.mu, p.Q, p.Nlx, p.Nly, p.Ltrot, p.beta,
+                            p.Nwrap, 1, 1, nullptr};
+  z2_options opt{0, 0, device, p.is_tau ? 1 : 0, 1, nullptr};
+  z2_handle *h = nullptr;
+  int r = z2_create(&h, cp.data(), nch, &opt);
+  if (r) return fail(h, "z2_create", r);
+  for (int c = 0; c < nch; ++c)
+    if ((r = z2_set_config(h, c, sig[c].data(), (int32_t)iseed[c]))) return fail(h, "z2_set_config", r);
+  if ((r = z2_pre(h))) return fail(h, "z2_pre", r);
+  const char *names[7] = {"flux_avg", "chi_flux", "pair_sc_q0", "cdw_pi", "cdw_shift", "cdw_ratio", "density"};
+  std::vector<double> tau((size_t)7 * N * p.Ltrot), tau_sum;
+  for (int nbc = 1; nbc <= p.Nbin; ++nbc) {
+    const bool istau = p.is_tau && nbc > p.Nthermal;
+    if ((r = z2_sweep(h, p.Nsweep, istau ? 1 : 0))) return fail(h, "z2_sweep", r);
+    double mean[7] = {0};
+    for (int c = 0; c < nch; ++c) {
+      double o[Z2_NOBS_EQ];
+      z2_get_obs_equal(h, c, o);
+      for (int q = 0; q < 7; ++q) mean[q] += o[q] / nch;
+    }
+    for (int q = 0; q < 7; ++q) if (q != 4) append(dir, names[q], mean[q]);
+    if (istau) {   // raw time-displaced correlators, averaged over chains
+      tau_sum.assign(tau.size(), 0.0);
+      for (int c = 0; c < nch; ++c) {
+        z2_get_obs_tau(h, c, tau.data());
+        for (size_t i = 0; i < tau.size(); ++i) tau_sum[i] += tau[i] / nch;
+      }
+      FILE *f = std::fopen((dir + "/obs_tau_raw").c_str(), "a");
+      if (f) { for (double v : tau_sum) std::fprintf(f, " %25.17E\n", v); std::fclose(f); }
+    }
+    if (nbc % 20 == 0 && info) {
+      double acc = 0;
+      for (int c = 0; c < nch; ++c) { double st[Z2_NSTATS]; z2_get_stats(h, c, st); acc += st[0]; }
+      std::fprintf(info, " Progress %d : Accept_Klocal_shift: %.17g\n", nbc, acc / (nch * nbc));
+    }
+  }
+  double acc = 0, xmax = 0, xmean = 0;
+  for (int c = 0; c < nch; ++c) {
+    double st[Z2_NSTATS];
+    z2_get_stats(h, c, st);
+    acc += st[0]; xmax = std::max(xmax, st[1]); xmean += st[2];
+  }
+  const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  if (info) {
+    std::fprintf(info, " Accept_Klocal_shift : %.17g\n", acc / (nch * p.Nbin));
+    std::fprintf(info, " Max diff Matrix     : %.17g\n", xmax);
+    std::fprintf(info, " Mean diff Matrix    : %.17g\n",
+                 xmean / (2.0 * nch * p.Nbin * (p.Ltrot / p.Nwrap) * p.Nsweep));
+    std::fprintf(info, " Tot CPU time        : %.10g\n", secs);
+    std::fclose(info);
+  }
+  // conf_out (src/fields.f90:509-557)
+  FILE *co = std::fopen((dir + "/confout.txt").c_str(), "w");
+  for (int c = 0; c < nch && co; ++c) {
+    std::vector<double> s((size_t)nb * p.Ltrot);
+    int32_t is = 0;
+    z2_get_config(h, c, s.data(), &is);
+    std::fprintf(co, " %d\n", is);
+    for (double v : s) std::fprintf(co, " %.1f\n", v);
+    for (int i = 0; i < N; ++i) std::fprintf(co, " 1.0\n");
+  }
+  if (co) std::fclose(co);
+  z2_destroy(h);
+  return 0;
+}
