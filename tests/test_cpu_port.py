@@ -1,0 +1,28 @@
+"""The C restatement (CPU baseline) agrees with the NumPy oracle: identical
+decisions and ranf state, G and observables to rounding."""
+import numpy as np
+
+from oracle import z2_oracle as zo
+from oracle import z2cpu
+
+
+def test_c_port_matches_python_oracle():
+    kw = dict(RT=1.0, J=0.5, h=0.5, mu=0.1, beta=2.0, Nlx=4, Nly=4, Ltrot=20, Nwrap=5)
+    out = z2cpu.run(**kw, seed=2024, nbins=2, record=True)
+    p = zo.Params(RT=1.0, J=0.5, h=0.5, mu=0.1, Nlx=4, Nly=4, Ltrot=20, beta=2.0, Nwrap=5)
+    c = zo.Z2Chain(p, seed=2024, record_decisions=True)
+    c.pre()
+    obs = []
+    for _ in range(2):
+        c.decisions = []
+        c.sweep()
+        d = c.obs.as_dict()
+        obs.append([d[k] for k in ("flux_avg", "chi_flux", "pair_sc_q0", "cdw_pi", "cdw_shift",
+                                   "cdw_ratio", "density")])
+    nb, L = 2 * p.Lq, p.Ltrot
+    dd = np.array(c.decisions, dtype=np.uint8).reshape(2, L, nb)
+    d_o = np.stack([dd[0][::-1, ::-1], dd[1]])
+    assert np.array_equal(out["decisions"], d_o)
+    assert out["iseed"] == c.rng.state
+    assert np.max(np.abs(out["G"] - c.prop.Gr)) < 1e-12
+    assert np.allclose(out["obs"], np.array(obs), rtol=1e-12, atol=1e-13)
