@@ -285,9 +285,9 @@ static int smem_small_bytes(int N) {
 }
 
 static int default_k(int N) {
-  if (N <= 36) return 32;
-  if (N <= 64) return 32;
-  if (N <= 100) return 16;
+  if (N <= 36) return 16;
+  if (N <= 64) return 16;
+  if (N <= 100) return 12;
   return 8;
 }
 
@@ -353,16 +353,16 @@ extern "C" int z2_create(z2_handle **out, const z2_chain_params *params, int32_t
     size_t nn = (size_t)N * ldg;
     int g_in = 0;
     int k2 = 2 * k;
-    if (nn + std::max<size_t>(2 * (size_t)(N | 1) * k2, kGemmTile) <= arena) g_in = 1;
-    else if (nn + std::max<size_t>(2 * (size_t)(N | 1) * 4, kGemmTile) <= arena) {
+    if (nn + std::max<size_t>(2 * (size_t)z2_ldx(N) * k2, kGemmTile) <= arena) g_in = 1;
+    else if (nn + std::max<size_t>(2 * (size_t)z2_ldx(N) * 4, kGemmTile) <= arena) {
       g_in = 1;
-      while (k2 > 4 && nn + 2 * (size_t)(N | 1) * k2 > arena) k2 -= 2;
+      while (k2 > 4 && nn + 2 * (size_t)z2_ldx(N) * k2 > arena) k2 -= 2;
     }
     if (!g_in) {
-      while (k2 > 2 && 2 * (size_t)(N | 1) * k2 > arena) k2 -= 2;
+      while (k2 > 2 && 2 * (size_t)z2_ldx(N) * k2 > arena) k2 -= 2;
     }
-    size_t need = small + 8 * (g_in ? nn + std::max<size_t>(2 * (size_t)(N | 1) * k2, kGemmTile)
-                                    : std::max<size_t>(2 * (size_t)(N | 1) * k2, kGemmTile));
+    size_t need = small + 8 * (g_in ? nn + std::max<size_t>(2 * (size_t)z2_ldx(N) * k2, kGemmTile)
+                                    : std::max<size_t>(2 * (size_t)z2_ldx(N) * k2, kGemmTile));
     smem_needed = std::max(smem_needed, (int)need);
     C.d = ChainDesc{};
     C.d.N = N; C.d.Lx = p.Nlx; C.d.Ly = p.Nly; C.d.Ltrot = p.Ltrot; C.d.Nwrap = p.Nwrap;
@@ -378,7 +378,7 @@ extern "C" int z2_create(z2_handle **out, const z2_chain_params *params, int32_t
     const int N = C.N;
     size_t arena = (h->smem - smem_small_bytes(N)) / 8;
     size_t nn = (size_t)N * C.d.ldg;
-    if (C.d.g_in_smem && nn + std::max<size_t>(2 * (size_t)(N | 1) * C.d.k2, kGemmTile) > arena)
+    if (C.d.g_in_smem && nn + std::max<size_t>(2 * (size_t)z2_ldx(N) * C.d.k2, kGemmTile) > arena)
       C.d.g_in_smem = 0;
   }
   CUDA_TRY(h, cudaFuncSetAttribute(z2_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -38,13 +38,13 @@ __device__ Smem make_smem(const ChainDesc &c, unsigned char *base, size_t smem_b
   const size_t nn = (size_t)N * c.ldg;
   if (c.g_in_smem) {
     s.G = s.arena; s.ldg = c.ldg;
-    s.ldx = N | 1; s.X = s.arena + nn; s.Yt = s.X + (size_t)s.ldx * c.k2;
+    s.ldx = z2_ldx(N); s.X = s.arena + nn; s.Yt = s.X + (size_t)s.ldx * c.k2;
     s.Wq = s.arena; s.ldq = c.ldg;
     s.tile = s.arena + nn;
     s.tile_doubles = (int)(arena_doubles - nn);
   } else {
     s.G = c.G; s.ldg = N;
-    s.ldx = N | 1; s.X = s.arena; s.Yt = s.X + (size_t)s.ldx * c.k2;
+    s.ldx = z2_ldx(N); s.X = s.arena; s.Yt = s.X + (size_t)s.ldx * c.k2;
     s.Wq = c.W4;
     s.ldq = N;
     s.tile = s.arena;
@@ -77,7 +77,11 @@ __device__ __noinline__ void build_table(const ChainDesc &c, const Smem &s, int 
 template <bool ROWS>
 __device__ __forceinline__ void kin_group_vec(const Smem &s, double *base, size_t stride, int g0,
                                               int half, double fl) {
-  const int2 *tp2 = reinterpret_cast<const int2 *>(s.tp);
+  // table pointers in registers (the Smem struct itself lives on the stack and
+  // would be re-read after every store)
+  const int2 *__restrict__ tp2 = reinterpret_cast<const int2 *>(s.tp);
+  const double *__restrict__ tc = s.tc;
+  const double *__restrict__ ts = s.ts;
   int kq = 0;
   for (; kq + 7 < half; kq += 8) {
     int2 pp[8];
@@ -85,8 +89,8 @@ __device__ __forceinline__ void kin_group_vec(const Smem &s, double *base, size_
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
       pp[q] = tp2[g0 + kq + q];
-      C[q] = s.tc[g0 + kq + q];
-      S[q] = fl * s.ts[g0 + kq + q];
+      C[q] = tc[g0 + kq + q];
+      S[q] = fl * ts[g0 + kq + q];
     }
 #pragma unroll
     for (int q = 0; q < 8; ++q) { a[q] = base[pp[q].x * stride]; b[q] = base[pp[q].y * stride]; }
@@ -98,7 +102,7 @@ __device__ __forceinline__ void kin_group_vec(const Smem &s, double *base, size_
   }
   for (; kq < half; ++kq) {
     const int2 pp = tp2[g0 + kq];
-    const double C = s.tc[g0 + kq], S = fl * s.ts[g0 + kq];
+    const double C = tc[g0 + kq], S = fl * ts[g0 + kq];
     const double a = base[pp.x * stride], b = base[pp.y * stride];
     base[pp.x * stride] = C * a + S * b;
     base[pp.y * stride] = S * a + C * b;
@@ -334,7 +338,12 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
   }
   __syncthreads();
   double *pdat = s.red + 48;      // accepted proposal: pinv(4), D11, D12
+  const int *__restrict__ bond = s.bond;
+  volatile int *flag = s.flag;
   unsigned int st = 0;
+  // 48828125^(lane+1) mod 2^31 in a register: lane L draws the (L+1)-th
+  // number of the batch without a divergent constant-memory read
+  const unsigned long long ipl = c_ipow[lane + 1];
   long long rpos = 0;
   int den = 0, num = 0;
   if (warp == 0) {
@@ -347,7 +356,7 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
       const int kk = done + lane;
       const bool valid = kk < nb;
       const int b = valid ? (descending ? nb - 1 - kk : kk) : 0;
-      const int p1 = s.bond[2 * b], p2 = s.bond[2 * b + 1];
+      const int p1 = bond[2 * b], p2 = bond[2 * b + 1];
       double g11 = G[p1 + (size_t)p1 * ldg], g12 = G[p1 + (size_t)p2 * ldg];
       double g21 = G[p2 + (size_t)p1 * ldg], g22 = G[p2 + (size_t)p2 * ldg];
       for (int q = 0; q < m; ++q) {
@@ -377,7 +386,8 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
       const double ratio = __dmul_rn(__dmul_rn(det, det), c.rb[is * 3 + it]);
       double r;
       if (c.replay && rpos + lane < c.nreplay) r = c.replay[rpos + lane];
-      else r = (double)ranf_adv(st, lane + 1) * (1.0 / 2147483648.0);
+      else r = (double)(unsigned int)(((unsigned long long)st * ipl) & 0x7fffffffull) *
+               (1.0 / 2147483648.0);
       const bool acc = valid && (fabs(ratio) > r);
       const unsigned ball = __ballot_sync(Z2_FULL, acc);
       const int first = ball ? (__ffs(ball) - 1) : 32;
@@ -391,7 +401,7 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
       if (lane == first) {
         pdat[0] = p22 / det; pdat[1] = -p12 / det; pdat[2] = -p21 / det; pdat[3] = p11 / det;
         pdat[4] = D11; pdat[5] = D12;
-        s.flag[1] = b;
+        flag[1] = b;
       }
       st = ranf_adv(st, cnt);
       rpos += cnt;
@@ -399,20 +409,21 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
       num += (first < 32) ? 1 : 0;
       __syncwarp();
       if (lane == 0) {
-        s.flag[0] = done + cnt;
-        if (first == 32) s.flag[1] = -1;
+        flag[0] = done + cnt;
+        if (first == 32) flag[1] = -1;
       }
     }
     __syncthreads();
-    done = s.flag[0];
-    const int b = s.flag[1];
+    done = flag[0];
+    const int b = flag[1];
     if (b >= 0) {
-      const int p1 = s.bond[2 * b], p2 = s.bond[2 * b + 1];
+      const int p1 = bond[2 * b], p2 = bond[2 * b + 1];
       const double q00 = pdat[0], q01 = pdat[1], q10 = pdat[2], q11 = pdat[3];
       const double D11 = pdat[4], D12 = pdat[5];
       for (int i = threadIdx.x; i < N; i += Z2_NT) {
         double u0 = G[i + (size_t)p1 * ldg], u1 = G[i + (size_t)p2 * ldg];
         double v0 = G[p1 + (size_t)i * ldg], v1 = G[p2 + (size_t)i * ldg];
+#pragma unroll 4
         for (int q = 0; q < m; ++q) {
           const double xi = X[i + (size_t)q * ldx], yi = Yt[i + (size_t)q * ldx];
           u0 -= xi * Yt[p1 + (size_t)q * ldx];

@@ -161,6 +161,11 @@ __device__ __forceinline__ void blk_sum_n(double *v, double *red) {
 
 __device__ __forceinline__ long long ph_now() { return clock64(); }
 
+// Leading dimension of the delayed-update factors X, Yt: = 8 (mod 16), so the
+// 8 rows x 4 columns of a DMMA A/B fragment fall on distinct shared-memory
+// bank pairs (two wavefronts per fragment load).
+__host__ __device__ __forceinline__ int z2_ldx(int N) { return ((N + 15) & ~15) + 8; }
+
 // ranf multiplier powers IP^i mod 2^31, i = 0..32 (filled by the host).
 __constant__ unsigned int c_ipow[33];
 
