@@ -118,8 +118,10 @@ int z2_set_replay(z2_handle *h, int32_t chain, const double *r, size_t n);
  * z2_create, accumulated over all z2_sweep calls (no reference counterpart;
  * the reference only records total wall time, src/main.f90:27-28,114-122).
  * out[Z2_NPHASE]: checkerboard wrap of G, proposals, rank-2k flushes,
- * equal-time observables, wraps + stabilization, time-displaced chain. */
-#define Z2_NPHASE 8
+ * equal-time observables, wraps + stabilization, time-displaced chain, and
+ * nested in those: UDV stabilization, stabilized G, flip-ratio rounds,
+ * accepted-flip X/Y columns, pending slice products, UDV stack copies. */
+#define Z2_NPHASE 12
 int z2_get_phase_cycles(const z2_handle *h, int32_t chain, double out[Z2_NPHASE]);
 int z2_get_decisions(const z2_handle *h, int32_t chain, uint8_t *dec,
                      double *ratios, size_t n);

@@ -26,7 +26,8 @@ from ._ffi import ChainParams, Options, Z2Error, dptr, fmat
 OBS_EQ_NAMES = ("flux_avg", "chi_flux", "pair_sc_q0", "cdw_pi", "cdw_shift", "cdw_ratio",
                 "density")
 OBS_TAU_NAMES = ("spin", "single", "pair_d", "pair_s", "charge_d", "charge_s", "curxx")
-PHASE_NAMES = ("kin", "propose", "flush", "obs_equal", "wrap_stab", "dyn", "stab_U", "stab_green")
+PHASE_NAMES = ("kin", "propose", "flush", "obs_equal", "wrap_stab", "dyn", "stab_U", "stab_green",
+               "eval", "cols", "pending", "stack")
 STAT_NAMES = ("acc", "Xmaxm", "Xmeanm", "Xmaxm_tau0", "Xmaxm_tau1", "Xmaxm_tau2",
               "Xmeanm_tau0", "Xmeanm_tau1", "Xmeanm_tau2", "accepted", "proposed", "draws",
               "nobs", "nobst")
@@ -181,7 +182,7 @@ class Z2Batch:
 
     def phase_cycles(self, chain: int) -> dict:
         """SM cycles per phase accumulated since creation (tracing)."""
-        buf = np.empty(8)
+        buf = np.empty(len(PHASE_NAMES))
         self._c(self.lib.z2_get_phase_cycles(self.h, chain, dptr(buf)))
         return dict(zip(PHASE_NAMES, buf.tolist()))
 

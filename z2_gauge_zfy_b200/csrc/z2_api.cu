@@ -13,6 +13,8 @@
 #include "../../include/z2dqmc.h"
 #include "z2_drivers.cuh"
 
+static_assert(PH_COUNT == Z2_NPHASE, "phase counters and the C ABI disagree");
+
 enum { OP_PRE = 1, OP_SWEEP = 2, OP_LOGDET = 3 };
 enum { U_MMULT_R = 1, U_MMULT_L, U_STAB_UR, U_STAB_UL, U_STAB_GREEN, U_STAB_GREEN_BIG };
 
@@ -41,6 +43,7 @@ z2_chain_kernel(const ChainDesc *descs, const int *order, int nchains, int *queu
                 int nsweep, int toggle, unsigned smem_bytes) {
   extern __shared__ __align__(16) unsigned char z2_smem[];
   __shared__ ChainDesc sc;
+  __shared__ Smem s;     // pointer table in shared memory, not on the local stack
   __shared__ int s_idx;
   for (;;) {
     if (threadIdx.x == 0) s_idx = atomicAdd(queue, 1);
@@ -48,7 +51,8 @@ z2_chain_kernel(const ChainDesc *descs, const int *order, int nchains, int *queu
     const int idx = s_idx;
     if (idx >= nchains) break;
     load_desc(sc, descs + order[idx]);
-    Smem s = make_smem(sc, z2_smem, smem_bytes);
+    if (threadIdx.x == 0) s = make_smem(sc, z2_smem, smem_bytes);
+    __syncthreads();
     if (op == OP_PRE) {
       for (int i = threadIdx.x; i < 2 * sc.nb; i += Z2_NT) s.bond[i] = sc.bonds[i];
       __syncthreads();
@@ -67,8 +71,10 @@ __global__ void __launch_bounds__(Z2_NT, 1)
 z2_unit_kernel(const ChainDesc *desc, int op, UnitArgs a, unsigned smem_bytes) {
   extern __shared__ __align__(16) unsigned char z2_smem[];
   __shared__ ChainDesc sc;
+  __shared__ Smem s;
   load_desc(sc, desc);
-  Smem s = make_smem(sc, z2_smem, smem_bytes);
+  if (threadIdx.x == 0) s = make_smem(sc, z2_smem, smem_bytes);
+  __syncthreads();
   const int N = sc.N;
   if (op == U_MMULT_R || op == U_MMULT_L) {
     build_table(sc, s, a.nt);

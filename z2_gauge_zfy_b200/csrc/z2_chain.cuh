@@ -77,8 +77,8 @@ __device__ __noinline__ void build_table(const ChainDesc &c, const Smem &s, int 
 template <bool ROWS>
 __device__ __forceinline__ void kin_group_vec(const Smem &s, double *base, size_t stride, int g0,
                                               int half, double fl) {
-  // table pointers in registers (the Smem struct itself lives on the stack and
-  // would be re-read after every store)
+  // table pointers in registers (the Smem struct would otherwise be re-read
+  // after every store, which may alias it)
   const int2 *__restrict__ tp2 = reinterpret_cast<const int2 *>(s.tp);
   const double *__restrict__ tc = s.tc;
   const double *__restrict__ ts = s.ts;
@@ -351,7 +351,9 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
     if (c.replay) rpos = *c.replay_pos;
   }
   int m = 0, done = 0;
+  long long t_eval = 0, t_cols = 0;
   while (done < nb) {
+    const long long t0 = ph_now();
     if (warp == 0) {
       const int kk = done + lane;
       const bool valid = kk < nb;
@@ -414,6 +416,8 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
       }
     }
     __syncthreads();
+    const long long t1 = ph_now();
+    t_eval += t1 - t0;
     done = flag[0];
     const int b = flag[1];
     if (b >= 0) {
@@ -447,6 +451,7 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
         sg[b] = sn;
       }
       __syncthreads();
+      t_cols += ph_now() - t1;
       m += 2;
       if (m >= k2) {
         const long long tf = ph_now();
@@ -467,6 +472,8 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
     c.acc[A_ACC_DEN] += (double)den;
     c.acc[A_DRAWS] += (double)den;
     c.acc[A_ACC_NUM] += (double)num;
+    c.acc[A_PH0 + PH_EVAL] += (double)t_eval;
+    c.acc[A_PH0 + PH_COLS] += (double)t_cols;
   }
   __syncthreads();
 }
@@ -620,13 +627,14 @@ __device__ __noinline__ void wrap_pre(const ChainDesc &c, const Smem &s, int nt,
   const int st = nt / c.Nwrap;
   if (nt != 0) {
     blk_copy(A, lda, c.UR, N, N, N);
-    apply_pending_R(c, s, A, lda, pd.lo, pd.hi, c.use_kin != 0);
+    { PhTimer t(c, PH_PEND); apply_pending_R(c, s, A, lda, pd.lo, pd.hi, c.use_kin != 0); }
     dev_stab_U(s, N, A, lda, c.UR, c.DR, c.VR, c.W0, false);
   }
   pd.lo = 1; pd.hi = 0;
-  blk_copy(c.URs + (size_t)st * NN, N, c.UR, N, N, N);
-  blk_copy(c.VRs + (size_t)st * NN, N, c.VR, N, N, N);
-  copy_vec(c.DRs + (size_t)st * N, c.DR, N);
+  { PhTimer t(c, PH_STACK);
+    blk_copy(c.URs + (size_t)st * NN, N, c.UR, N, N, N);
+    blk_copy(c.VRs + (size_t)st * NN, N, c.VR, N, N, N);
+    copy_vec(c.DRs + (size_t)st * N, c.DR, N); }
   if (nt == c.Ltrot) {
     dev_stab_green(s, N, nt, c.Ltrot, c.UR, c.DR, c.VR, c.ULT, c.DL, c.VL, A, lda, c.W1, c.W2,
                    c.W0, c.G);
@@ -639,29 +647,31 @@ __device__ __noinline__ void wrap_L(const ChainDesc &c, const Smem &s, int nt, P
   spill_G(c, s);
   int lda; double *A = qr_matrix(c, s, lda);
   const int st = nt / c.Nwrap;
-  blk_copy(c.UR, N, c.URs + (size_t)st * NN, N, N, N);
-  blk_copy(c.VR, N, c.VRs + (size_t)st * NN, N, N, N);
-  copy_vec(c.DR, c.DRs + (size_t)st * N, N);
+  { PhTimer t(c, PH_STACK);
+    blk_copy(c.UR, N, c.URs + (size_t)st * NN, N, N, N);
+    blk_copy(c.VR, N, c.VRs + (size_t)st * NN, N, N, N);
+    copy_vec(c.DR, c.DRs + (size_t)st * N, N); }
   if (pd.lo <= pd.hi) {
     blk_copy(A, lda, c.ULT, N, N, N);
-    apply_pending_L(c, s, A, lda, pd.lo, pd.hi);
+    { PhTimer t(c, PH_PEND); apply_pending_L(c, s, A, lda, pd.lo, pd.hi); }
     if (nt == c.Ltrot) blk_copy(c.ULT, N, A, lda, N, N);
   } else if (nt != c.Ltrot) {
     blk_copy(A, lda, c.ULT, N, N, N);
   }
   pd.lo = 1; pd.hi = 0;
   if (nt != c.Ltrot) {
-    { PhTimer t(c, 6); dev_stab_U(s, N, A, lda, c.ULT, c.DL, c.VL, c.W0, true); }
-    { PhTimer t(c, 7);
+    { PhTimer t(c, PH_STABU); dev_stab_U(s, N, A, lda, c.ULT, c.DL, c.VL, c.W0, true); }
+    { PhTimer t(c, PH_STABG);
       dev_stab_green(s, N, nt, c.Ltrot, c.UR, c.DR, c.VR, c.ULT, c.DL, c.VL, A, lda, c.W1, c.W2,
                      c.W0, c.W3); }
     double dif = blk_maxdiff(c.W3, N, c.G, N, N, s.red);
     record_drift(c, dif, stats);
     blk_copy(c.G, N, c.W3, N, N, N);
   }
-  blk_copy(c.ULTs + (size_t)st * NN, N, c.ULT, N, N, N);
-  blk_copy(c.VLs + (size_t)st * NN, N, c.VL, N, N, N);
-  copy_vec(c.DLs + (size_t)st * N, c.DL, N);
+  { PhTimer t(c, PH_STACK);
+    blk_copy(c.ULTs + (size_t)st * NN, N, c.ULT, N, N, N);
+    blk_copy(c.VLs + (size_t)st * NN, N, c.VL, N, N, N);
+    copy_vec(c.DLs + (size_t)st * N, c.DL, N); }
   load_G(c, s);
 }
 
@@ -671,29 +681,31 @@ __device__ __noinline__ void wrap_R(const ChainDesc &c, const Smem &s, int nt, P
   spill_G(c, s);
   int lda; double *A = qr_matrix(c, s, lda);
   const int st = nt / c.Nwrap;
-  blk_copy(c.ULT, N, c.ULTs + (size_t)st * NN, N, N, N);
-  blk_copy(c.VL, N, c.VLs + (size_t)st * NN, N, N, N);
-  copy_vec(c.DL, c.DLs + (size_t)st * N, N);
+  { PhTimer t(c, PH_STACK);
+    blk_copy(c.ULT, N, c.ULTs + (size_t)st * NN, N, N, N);
+    blk_copy(c.VL, N, c.VLs + (size_t)st * NN, N, N, N);
+    copy_vec(c.DL, c.DLs + (size_t)st * N, N); }
   if (pd.lo <= pd.hi) {
     blk_copy(A, lda, c.UR, N, N, N);
-    apply_pending_R(c, s, A, lda, pd.lo, pd.hi, true);
+    { PhTimer t(c, PH_PEND); apply_pending_R(c, s, A, lda, pd.lo, pd.hi, true); }
     if (nt == 0) blk_copy(c.UR, N, A, lda, N, N);
   } else if (nt != 0) {
     blk_copy(A, lda, c.UR, N, N, N);
   }
   pd.lo = 1; pd.hi = 0;
   if (nt != 0) {
-    { PhTimer t(c, 6); dev_stab_U(s, N, A, lda, c.UR, c.DR, c.VR, c.W0, false); }
-    { PhTimer t(c, 7);
+    { PhTimer t(c, PH_STABU); dev_stab_U(s, N, A, lda, c.UR, c.DR, c.VR, c.W0, false); }
+    { PhTimer t(c, PH_STABG);
       dev_stab_green(s, N, nt, c.Ltrot, c.UR, c.DR, c.VR, c.ULT, c.DL, c.VL, A, lda, c.W1, c.W2,
                      c.W0, c.W3); }
     double dif = blk_maxdiff(c.W3, N, c.G, N, N, s.red);
     record_drift(c, dif, stats);
     blk_copy(c.G, N, c.W3, N, N, N);
   }
-  blk_copy(c.URs + (size_t)st * NN, N, c.UR, N, N, N);
-  blk_copy(c.VRs + (size_t)st * NN, N, c.VR, N, N, N);
-  copy_vec(c.DRs + (size_t)st * N, c.DR, N);
+  { PhTimer t(c, PH_STACK);
+    blk_copy(c.URs + (size_t)st * NN, N, c.UR, N, N, N);
+    blk_copy(c.VRs + (size_t)st * NN, N, c.VR, N, N, N);
+    copy_vec(c.DRs + (size_t)st * N, c.DR, N); }
   load_G(c, s);
 }
 

@@ -24,14 +24,17 @@ enum {
   A_BIN0,                        // 7 bin results: flux_avg .. density
   A_LOGDET = A_BIN0 + 7, A_DMU, A_DRAWS,
   A_PH0,                         // Z2_NPHASE per-phase SM cycle counters
-  A_COUNT = A_PH0 + 8
+  A_COUNT = A_PH0 + 12
 };
 
 // Phases of a bin timed with clock64() by thread 0 (tracing; no effect on
 // results): checkerboard wrap of G, proposals (evaluation + rank-2 bookkeeping),
 // rank-2k flushes, equal-time observables, wraps/stabilization, the
-// time-displaced chain.
-enum { PH_KIN = 0, PH_PROP, PH_FLUSH, PH_OBS, PH_WRAP, PH_DYN, PH_COUNT = 8 };
+// time-displaced chain; inside those: the UDV stabilization, the stabilized
+// Green's function, warp-0 flip-ratio rounds, the accepted-flip columns of X
+// and Y, the pending slice products of a wrap, and the UDV stack copies.
+enum { PH_KIN = 0, PH_PROP, PH_FLUSH, PH_OBS, PH_WRAP, PH_DYN, PH_STABU, PH_STABG,
+       PH_EVAL, PH_COLS, PH_PEND, PH_STACK, PH_COUNT = 12 };
 
 // Status flags (ChainDesc::status).
 enum { ST_NONFINITE = 1, ST_BADARG = 2 };

@@ -240,6 +240,117 @@ __device__ __noinline__ void blk_org2r_tc(double *A, int lda, int m, int n, cons
   }
 }
 
+// DORGQR for a square n x n matrix with n reflectors, blocked: blocks of nb
+// reflectors from the last to the first, each applied as the compact WY form
+// H_i0 ... H_i0+ib-1 = I - V T V^T (DLARFT forward/columnwise) by DMMA GEMMs:
+//   trailing columns  C <- C - V (T (V^T C)),
+//   block columns     A(i0:, i0:i0+ib) = E - V (T V1^T),  rows above = 0.
+// work (shared memory, wd doubles) holds V (ldv x nb, ldv = 4 mod 16 so both
+// DMMA fragment orientations are bank-conflict free) and W (ldw x (n - nb),
+// ldw odd for the thread-per-column T W product); T and the Gram matrix
+// (nb x nb each) go to small (sd doubles) when it is large enough, else to
+// work.  When work is too small the unblocked DORG2R runs instead (same Q up
+// to rounding).
+__device__ __noinline__ void blk_orgqr(double *A, int lda, int n, const double *tau, double *work,
+                                      int wd, double *small, int sd) {
+  const int ldv = ((n + 11) & ~15) + 4;
+  int nb = 16;
+  auto need = [n, ldv, sd](int b) {
+    return ldv * b + (b + 1) * (n > b ? n - b : 0) + (2 * b * b <= sd ? 0 : 2 * b * b);
+  };
+  if (need(nb) > wd) nb = 8;
+  if (need(nb) > wd) {
+    blk_org2r_tc(A, lda, n, n, tau);
+    return;
+  }
+  const int ldw = nb + 1;
+  double *V = work;
+  double *W = V + (size_t)ldv * nb;
+  double *T = (2 * nb * nb <= sd) ? small : W + (size_t)ldw * (n > nb ? n - nb : 0);
+  double *S = T + nb * nb;
+  const int tid = threadIdx.x;
+  for (int i0 = ((n - 1) / nb) * nb; i0 >= 0; i0 -= nb) {
+    const int ib = (n - i0) < nb ? (n - i0) : nb;
+    const int mp = n - i0, nc = n - i0 - ib;
+    // V: unit lower trapezoidal, mp x ib
+    for (int e = tid; e < mp * ib; e += Z2_NT) {
+      const int r = e % mp, c = e / mp;
+      V[r + (size_t)c * ldv] = (r == c) ? 1.0 : (r > c ? A[(i0 + r) + (size_t)(i0 + c) * lda] : 0.0);
+    }
+    __syncthreads();
+    // S = V^T V
+    blk_dmma(ib, ib, mp, 1.0, MatRef{V, ldv, 1}, false, MatRef{V, 1, ldv}, false, 0.0, S, ib);
+    // T (DLARFT): T(c,c) = tau_c, T(r,c) = -tau_c sum_{r<=q<c} T(r,q) S(q,c).
+    // Row r depends only on itself, so thread r builds it in registers.
+    if (tid < ib) {
+      const int r = tid;
+      double tr[16];
+#pragma unroll
+      for (int c = 0; c < 16; ++c) {
+        double t = 0.0;
+        if (c < ib) {
+          if (c == r) {
+            t = tau[i0 + c];
+          } else if (c > r) {
+            double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+            for (int q = 0; q < c; ++q) {
+              if (q >= r) {
+                if (q & 1) a1 += tr[q] * S[q + c * ib];
+                else a0 += tr[q] * S[q + c * ib];
+              }
+            }
+            t = -tau[i0 + c] * (a0 + a1);
+          }
+        }
+        tr[c] = t;
+      }
+#pragma unroll
+      for (int c = 0; c < 16; ++c)
+        if (c < ib) T[r + c * ib] = tr[c];
+    }
+    __syncthreads();
+    if (nc > 0) {
+      double *C = A + i0 + (size_t)(i0 + ib) * lda;
+      // W = V^T C  (ib x nc, ld ldw)
+      blk_dmma(ib, nc, mp, 1.0, MatRef{V, ldv, 1}, false, MatRef{C, 1, lda}, false, 0.0, W, ldw);
+      // W <- T W, one thread per column
+      for (int j = tid; j < nc; j += Z2_NT) {
+        double w[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) w[q] = (q < ib) ? W[q + j * ldw] : 0.0;
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+          if (r < ib) {
+            double t = 0.0;
+#pragma unroll
+            for (int q = r; q < 16; ++q)
+              if (q < ib) t += T[r + q * ib] * w[q];
+            W[r + j * ldw] = t;
+          }
+        }
+      }
+      __syncthreads();
+      // C -= V W
+      blk_dmma(mp, nc, ib, -1.0, MatRef{V, 1, ldv}, false, MatRef{W, 1, ldw}, false, 1.0, C, lda);
+    }
+    // S <- T V1^T (ib x ib); block columns <- E - V S, rows above i0 <- 0
+    for (int e = tid; e < ib * ib; e += Z2_NT) {
+      const int r = e % ib, c = e / ib;
+      double t = 0.0;
+      for (int q = r; q <= c; ++q) t += T[r + q * ib] * V[c + (size_t)q * ldv];
+      S[r + c * ib] = t;
+    }
+    for (int e = tid; e < n * ib; e += Z2_NT) {
+      const int r = e % n, c = e / n;
+      A[r + (size_t)(i0 + c) * lda] = (r == i0 + c) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    blk_dmma(mp, ib, ib, -1.0, MatRef{V, 1, ldv}, false, MatRef{S, 1, ib}, false, 1.0,
+             A + i0 + (size_t)i0 * lda, lda);
+  }
+}
+
 // Solve R Z = Y in place (DTRSM 'L','U','N','N'), Y n x nc (ldy), R upper
 // (ldr).  Blocks of 8 rows from the bottom: the 8 x 8 diagonal block is
 // solved one thread per column (block of R held in registers), the rows
