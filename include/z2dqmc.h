@@ -123,6 +123,16 @@ int z2_set_replay(z2_handle *h, int32_t chain, const double *r, size_t n);
  * accepted-flip X/Y columns, pending slice products, UDV stack copies. */
 #define Z2_NPHASE 12
 int z2_get_phase_cycles(const z2_handle *h, int32_t chain, double out[Z2_NPHASE]);
+/* Delay-rank autotuner (no reference counterpart: the reference applies each
+ * accepted flip to G at once, src/localK.f90:141-165).  For every distinct
+ * lattice size among params[0..nchains) it times one bin of short probe
+ * chains (the chain's couplings and time step, Ltrot cut to 2*Nwrap) at the
+ * ranks 4, 6, 8, 12, 16, 24, 32, 48, 64 (capped by shared memory) and writes
+ * the fastest rank of each chain's size to k_out[nchains], ready to pass as
+ * z2_options.delay_k_chain.  Uses opt->device (opt may be NULL: device 0);
+ * allocates and frees its own probe handles. */
+int z2_tune_delay(const z2_chain_params *params, int32_t nchains, const z2_options *opt,
+                  int32_t *k_out);
 int z2_get_decisions(const z2_handle *h, int32_t chain, uint8_t *dec,
                      double *ratios, size_t n);
 

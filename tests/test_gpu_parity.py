@@ -271,3 +271,24 @@ def test_graph_replay_and_delay_rank_identical_decisions():
         g2, d2, s2 = outs[2][i]
         assert np.array_equal(d0, d2) and np.array_equal(s0, s2)
         assert rel(g2, g0) < RTOL
+
+
+def test_delay_autotuner():
+    """z2_tune_delay gives one rank per lattice size from its candidate list,
+    and a batch built with the tuned ranks makes the same decisions."""
+    from z2_gauge_zfy_b200 import tune_delay
+    chains = [Chain(RT=1.0, J=0.5, h=0.5, Nlx=L, Nly=L, Ltrot=20, beta=2.0, Nwrap=10, seed=s)
+              for L, s in ((4, 21), (6, 22), (4, 23), (6, 24))]
+    k = tune_delay(chains)
+    assert k.shape == (4,)
+    assert set(k.tolist()) <= {4, 6, 8, 12, 16, 24, 32, 48, 64}
+    assert k[0] == k[2] and k[1] == k[3]
+    outs = []
+    for kw in (dict(), dict(delay_k="auto")):
+        with Z2Batch(chains, record=True, **kw) as b:
+            b.pre()
+            b.sweep(2, False)
+            outs.append([(b.green(i), b.decisions(i)[0]) for i in range(4)])
+    for (g0, d0), (g1, d1) in zip(*outs):
+        assert np.array_equal(d0, d1)
+        assert rel(g1, g0) < RTOL

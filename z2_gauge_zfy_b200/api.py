@@ -62,28 +62,57 @@ def _check(lib, h, code):
         raise Z2Error(code, msg.decode() if msg else "")
 
 
+def _params(chains):
+    """ctypes array of z2_chain_params (and the per-bond arrays it points to)."""
+    n = len(chains)
+    arr = (ChainParams * n)()
+    keep = []
+    for i, ch in enumerate(chains):
+        p = arr[i]
+        p.RT, p.J, p.h, p.mu, p.Q = ch.RT, ch.J, ch.h, ch.mu, ch.Q
+        p.Nlx, p.Nly, p.Ltrot, p.beta = ch.Nlx, ch.Nly, ch.Ltrot, ch.beta
+        p.Nwrap, p.absolute, p.seed = ch.Nwrap, ch.absolute, ch.seed
+        if ch.rt_bond is not None:
+            rb = np.ascontiguousarray(ch.rt_bond, dtype=np.float64)
+            assert rb.shape == (2 * ch.N,)
+            keep.append(rb)
+            p.rt_bond = dptr(rb)
+        else:
+            p.rt_bond = None
+    return arr, keep
+
+
+def tune_delay(chains, device: int = 0) -> np.ndarray:
+    """Per-chain delayed-update rank picked by the library's autotuner
+    (``z2_tune_delay``: short probe chains of each lattice size, timed at
+    every candidate rank on the GPU)."""
+    lib = _ffi.load()
+    chains = list(chains)
+    arr, _keep = _params(chains)
+    opt = Options(0, 0, device, 0, 0, None)
+    k = np.zeros(len(chains), dtype=np.int32)
+    code = lib.z2_tune_delay(arr, len(chains), C.byref(opt),
+                             k.ctypes.data_as(C.POINTER(C.c_int32)))
+    if code != 0:
+        raise Z2Error(code, "z2_tune_delay failed")
+    return k
+
+
 class Z2Batch:
     """A batch of chains resident on one GPU (``z2_create``)."""
 
-    def __init__(self, chains, delay_k: int = 0, record: bool = False, device: int = 0,
+    def __init__(self, chains, delay_k=0, record: bool = False, device: int = 0,
                  tau: bool = False, graph: bool = False, delay_k_chain=None):
+        """delay_k: rank of the delayed updates for every chain (0 = built-in
+        default per lattice size), or "auto" to run the autotuner
+        (``z2_tune_delay``) and use its per-chain ranks."""
         self.lib = _ffi.load()
         self.chains = list(chains)
         n = len(self.chains)
-        arr = (ChainParams * n)()
-        self._rt_keep = []
-        for i, ch in enumerate(self.chains):
-            p = arr[i]
-            p.RT, p.J, p.h, p.mu, p.Q = ch.RT, ch.J, ch.h, ch.mu, ch.Q
-            p.Nlx, p.Nly, p.Ltrot, p.beta = ch.Nlx, ch.Nly, ch.Ltrot, ch.beta
-            p.Nwrap, p.absolute, p.seed = ch.Nwrap, ch.absolute, ch.seed
-            if ch.rt_bond is not None:
-                rb = np.ascontiguousarray(ch.rt_bond, dtype=np.float64)
-                assert rb.shape == (2 * ch.N,)
-                self._rt_keep.append(rb)
-                p.rt_bond = dptr(rb)
-            else:
-                p.rt_bond = None
+        arr, self._rt_keep = _params(self.chains)
+        if delay_k == "auto":
+            delay_k_chain = tune_delay(self.chains, device)
+            delay_k = 0
         self._kc = None
         kc_ptr = None
         if delay_k_chain is not None:

@@ -756,6 +756,87 @@ extern "C" int z2_get_phase_cycles(const z2_handle *h, int32_t chain, double out
   return Z2_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Delay-rank autotuner.  The reference applies every accepted flip to G at
+// once (src/localK.f90:141-165); here flips are queued and flushed as one
+// rank-2k GEMM, and the best k trades the flush GEMM's efficiency (grows with
+// k) against the per-proposal corrections and the column build (grow with
+// k).  For each distinct lattice size the tuner runs short probe chains with
+// the chain's own couplings and time step (Ltrot cut to 2 Nwrap) at every
+// candidate rank, all sizes side by side in one persistent launch per
+// candidate, and keeps the rank with the fewest SM cycles per bin.
+// ---------------------------------------------------------------------------
+static const int kTuneCand[] = {4, 6, 8, 12, 16, 24, 32, 48, 64};
+
+extern "C" int z2_tune_delay(const z2_chain_params *params, int32_t nchains,
+                             const z2_options *opt, int32_t *k_out) {
+  if (!params || nchains <= 0 || !k_out) return Z2_ERR_ARG;
+  const int reps = 2;
+  // one representative chain per distinct N
+  std::vector<int> sizes, rep;
+  for (int c = 0; c < nchains; ++c) {
+    const int N = params[c].Nlx * params[c].Nly;
+    if (std::find(sizes.begin(), sizes.end(), N) == sizes.end()) {
+      sizes.push_back(N);
+      rep.push_back(c);
+    }
+  }
+  const int ns = (int)sizes.size();
+  std::vector<z2_chain_params> probe;
+  for (int i = 0; i < ns; ++i) {
+    z2_chain_params p = params[rep[i]];
+    const double dtau = p.beta / (double)p.Ltrot;
+    const int Lt = std::min(p.Ltrot, 2 * p.Nwrap);
+    p.beta = dtau * Lt;
+    p.Ltrot = Lt;
+    for (int r = 0; r < reps; ++r) {
+      z2_chain_params q = p;
+      q.seed = p.seed + 7919 * r;
+      probe.push_back(q);
+    }
+  }
+  std::vector<double> best(ns, 1e300);
+  std::vector<int> bestk(ns, 0), lastk(ns, -1);
+  for (int k : kTuneCand) {
+    z2_options o{};
+    o.delay_k = k;
+    o.device = opt ? opt->device : 0;
+    z2_handle *h = nullptr;
+    int rc = z2_create(&h, probe.data(), (int)probe.size(), &o);
+    if (rc == Z2_OK) rc = z2_pre(h);
+    if (rc == Z2_OK) rc = z2_sweep(h, 1, 0);   // warm-up bin
+    std::vector<double> c0(probe.size() * Z2_NPHASE), c1(probe.size() * Z2_NPHASE);
+    for (int c = 0; rc == Z2_OK && c < (int)probe.size(); ++c)
+      rc = z2_get_phase_cycles(h, c, &c0[(size_t)c * Z2_NPHASE]);
+    if (rc == Z2_OK) rc = z2_sweep(h, 1, 0);
+    for (int c = 0; rc == Z2_OK && c < (int)probe.size(); ++c)
+      rc = z2_get_phase_cycles(h, c, &c1[(size_t)c * Z2_NPHASE]);
+    if (rc != Z2_OK) {
+      z2_destroy(h);
+      return rc;
+    }
+    for (int i = 0; i < ns; ++i) {
+      // the rank actually used (shared memory may cap it)
+      const int keff = h->ch[i * reps].d.k2 / 2;
+      if (keff == lastk[i]) continue;
+      lastk[i] = keff;
+      double cyc = 0.0;
+      for (int r = 0; r < reps; ++r) {
+        const size_t b = (size_t)(i * reps + r) * Z2_NPHASE;
+        for (int ph : {PH_KIN, PH_PROP, PH_OBS, PH_WRAP, PH_DYN}) cyc += c1[b + ph] - c0[b + ph];
+      }
+      if (cyc < best[i]) { best[i] = cyc; bestk[i] = keff; }
+    }
+    z2_destroy(h);
+  }
+  for (int c = 0; c < nchains; ++c) {
+    const int N = params[c].Nlx * params[c].Nly;
+    const int i = (int)(std::find(sizes.begin(), sizes.end(), N) - sizes.begin());
+    k_out[c] = bestk[i];
+  }
+  return Z2_OK;
+}
+
 static int upload_desc(z2_handle *h, int chain) {
   CUDA_TRY(h, cudaMemcpy(h->d_desc + chain, &h->ch[chain].d, sizeof(ChainDesc),
                          cudaMemcpyHostToDevice));
