@@ -30,6 +30,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 DTAU = 0.1
+# DRAM bytes (read + write) of one step of the 256-chain workload, from one
+# ncu capture of the chain kernel (dram__bytes_read.sum + dram__bytes_write.sum)
+TRAFFIC_BYTES_PER_STEP = 2817193728 + 4923897856
 
 
 def batched_chains(rank: int = 0, n: int = 256):
@@ -50,6 +53,35 @@ def single_chain():
     from z2_gauge_zfy_b200 import Chain
     return [Chain(RT=1.0, J=0.5, h=0.5, mu=0.0, Nlx=8, Nly=8, Ltrot=100, beta=10.0, Nwrap=10,
                   absolute=1, seed=12345)]
+
+
+def adjoint_cost(device: int) -> dict:
+    """Cost of the log-det adjoint (z2_logdet_grad) against one sweep of the
+    same chain, both timed end to end through the API (median of 3)."""
+    from z2_gauge_zfy_b200 import Chain, Z2Batch
+    L = 12
+    rng = np.random.default_rng(4)
+    rt = 1.0 + 0.05 * rng.standard_normal(2 * L * L)
+    ch = Chain(RT=1.0, J=0.5, h=0.5, mu=0.1, Nlx=L, Nly=L, Ltrot=120, beta=12.0, Nwrap=10,
+               seed=20250, rt_bond=rt)
+    with Z2Batch([ch], device=device) as b:
+        b.logdet_grad(0)
+        tg = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            b.logdet_grad(0)
+            tg.append(time.perf_counter() - t0)
+        b.pre()
+        b.sweep(1, False)
+        ts = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            b.sweep(1, False)
+            ts.append(time.perf_counter() - t0)
+    g, s_ = statistics.median(tg), statistics.median(ts)
+    return {"workload": "L=12 (N=144), beta=12, dtau 0.1, Ltrot 120, per-bond t = 1 + 0.05 N(0,1), "
+                        "mu=0.1, seeded +-1 links, gradient wrt 288 t_b and mu",
+            "logdet_grad_ms": g * 1e3, "sweep_ms": s_ * 1e3, "grad_over_sweep": g / s_}
 
 
 def site_updates(chains) -> int:
@@ -230,11 +262,16 @@ def main():
 
     import __graft_entry__
     __graft_entry__.build()
-    from z2_gauge_zfy_b200 import Z2Batch
+    from z2_gauge_zfy_b200 import Z2Batch, tune_delay
 
     chains = batched_chains(rank, args.chains)
     su_step = site_updates(chains)
-    b = Z2Batch(chains, device=local)
+    # delayed-update rank per lattice size from the library's autotuner
+    # (short probe chains, before the timed region)
+    t_tune = time.perf_counter()
+    kchain = tune_delay(chains, local)
+    t_tune = time.perf_counter() - t_tune
+    b = Z2Batch(chains, device=local, delay_k_chain=kchain)
     b.pre()
     for _ in range(args.warmup):
         b.sweep(1, False)
@@ -295,13 +332,18 @@ def main():
                    "chains_per_gpu": len(chains), "site_updates_per_step_per_gpu": su_step,
                    "parallelism": f"chains sharded over {world} GPU(s), replicas",
                    "l2": "inputs larger than L2 (per-GPU chain state > 126 MB)",
-                   "accept_rate": a_rate},
+                   "accept_rate": a_rate,
+                   "delay_rank": {str(c.N): int(k) for c, k in zip(chains, kchain)},
+                   "autotune_s": t_tune},
         "e2e": {"value": e2e, "unit": "site-updates/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": len(chains) * 7 * 8},
         "gpu_launches": args.steps,
         "clocks": clocks,
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak,
-                     "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                     "unit": "TFLOP/s", "frac": achieved / peak,
+                     "traffic": TRAFFIC_BYTES_PER_STEP if len(chains) == 256 else None,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                       "bench step (256 chains)",
                      "note": f"FP64 algorithmic flops per launch / launch time; peak {peak_kind}"},
     }
     b.close()
@@ -317,6 +359,8 @@ def main():
                                             "K=0.5, one chain", "value": sv,
                                 "unit": "site-updates/s",
                                 "batched_over_single_per_gpu": (value / world) / sv}
+    if rank == 0 and not args.no_single:
+        line["adjoint"] = adjoint_cost(local)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample()
     if rank == 0:
