@@ -1,7 +1,7 @@
 // z2_stab.cuh -- UDV stabilization (src/stabilization.f90:42-200) on the
-// DMMA GEMM, the thread-per-column pivoted QR and the blocked DORGQR.
+// DMMA GEMM, the register-resident pivoted QR and the blocked DORGQR.
 #pragma once
-#include "z2_dmma.cuh"
+#include "z2_qrp.cuh"
 
 // stab_UR (left = false) / stab_UL (left = true), src/stabilization.f90:70-120.
 // On entry A (lda; shared arena or global) holds the propagated U (UR, or
@@ -12,7 +12,7 @@ __device__ __noinline__ void dev_stab_U(const Smem &s, int N, double *A, int lda
   double *tau = s.vec, *vn1 = s.vec + N, *vn2 = s.vec + 2 * N, *Dn = s.vec + 3 * N;
   int *jpvt = s.ivec;
   blk_scale_cols(A, lda, N, N, D);                 // matUDV(:,i) *= D(i)
-  blk_geqp3_tc(A, lda, N, jpvt, tau, vn1, vn2);    // ZGEQP3
+  blk_geqp3_fast(A, lda, N, jpvt, tau, vn1, vn2, s.tile, s.tile_doubles, s.red);   // ZGEQP3
   blk_qdrp_scale(A, lda, N, Dn);                   // D = |R_ii|, R rows /= D
   for (int i = threadIdx.x; i < N; i += Z2_NT) D[i] = Dn[i];
   if (!left) {
@@ -67,7 +67,7 @@ __device__ __noinline__ void dev_stab_green(const Smem &s, int N, int nt, int Lt
     }
     __syncthreads();
   }
-  blk_geqp3_tc(M, ldm, N, jpvt, tau, vn1, vn2);
+  blk_geqp3_fast(M, ldm, N, jpvt, tau, vn1, vn2, s.tile, s.tile_doubles, s.red);
   blk_qdrp_scale(M, ldm, N, Dn);
   // keep the scaled R (upper triangle) for the triangular solve
   for (int j = threadIdx.x / 32; j < N; j += Z2_WARPS)
