@@ -361,10 +361,19 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
       const int p1 = bond[2 * b], p2 = bond[2 * b + 1];
       double g11 = G[p1 + (size_t)p1 * ldg], g12 = G[p1 + (size_t)p2 * ldg];
       double g21 = G[p2 + (size_t)p1 * ldg], g22 = G[p2 + (size_t)p2 * ldg];
-      for (int q = 0; q < m; ++q) {
-        const double xa = X[p1 + (size_t)q * ldx], xb = X[p2 + (size_t)q * ldx];
-        const double ya = Yt[p1 + (size_t)q * ldx], yb = Yt[p2 + (size_t)q * ldx];
-        g11 -= xa * ya; g12 -= xa * yb; g21 -= xb * ya; g22 -= xb * yb;
+      {
+        // m is even (two columns per accept): two independent FMA chains
+        double h11 = 0.0, h12 = 0.0, h21 = 0.0, h22 = 0.0;
+        const double *xp1 = X + p1, *xp2 = X + p2, *yp1 = Yt + p1, *yp2 = Yt + p2;
+#pragma unroll 2
+        for (int q = 0; q < m; q += 2) {
+          const size_t o0 = (size_t)q * ldx, o1 = o0 + ldx;
+          const double xa0 = xp1[o0], xb0 = xp2[o0], ya0 = yp1[o0], yb0 = yp2[o0];
+          const double xa1 = xp1[o1], xb1 = xp2[o1], ya1 = yp1[o1], yb1 = yp2[o1];
+          g11 -= xa0 * ya0; g12 -= xa0 * yb0; g21 -= xb0 * ya0; g22 -= xb0 * yb0;
+          h11 += xa1 * ya1; h12 += xa1 * yb1; h21 += xb1 * ya1; h22 += xb1 * yb1;
+        }
+        g11 -= h11; g12 -= h12; g21 -= h21; g22 -= h22;
       }
       const double s_old = (double)sig[b];
       const double s_new = -s_old;
@@ -378,6 +387,9 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
       const double m22 = __dadd_rn(__dmul_rn(D12, l12), __dmul_rn(D11, l22));
       const double p11 = __dadd_rn(1.0, m11), p12 = m12, p21 = m21, p22 = __dadd_rn(1.0, m22);
       const double det = __dsub_rn(__dmul_rn(p11, p22), __dmul_rn(p12, p21));
+      // Prod^-1 entries in every lane, ahead of the ballot (off the path of
+      // the accepting lane)
+      const double idet = 1.0 / det;
       // boson ratio (src/fields.f90:40-119) from the host table
       const short *bb = bbs + 6 * b;
       const double tmp_old = s_old * sig[bb[0]] * sig[bb[1]] * sig[bb[2]] +
@@ -401,7 +413,7 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
         if (c.ratios) c.ratios[li] = ratio;
       }
       if (lane == first) {
-        pdat[0] = p22 / det; pdat[1] = -p12 / det; pdat[2] = -p21 / det; pdat[3] = p11 / det;
+        pdat[0] = p22 * idet; pdat[1] = -p12 * idet; pdat[2] = -p21 * idet; pdat[3] = p11 * idet;
         pdat[4] = D11; pdat[5] = D12;
         flag[1] = b;
       }
@@ -427,13 +439,21 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
       for (int i = threadIdx.x; i < N; i += Z2_NT) {
         double u0 = G[i + (size_t)p1 * ldg], u1 = G[i + (size_t)p2 * ldg];
         double v0 = G[p1 + (size_t)i * ldg], v1 = G[p2 + (size_t)i * ldg];
-#pragma unroll 4
-        for (int q = 0; q < m; ++q) {
-          const double xi = X[i + (size_t)q * ldx], yi = Yt[i + (size_t)q * ldx];
-          u0 -= xi * Yt[p1 + (size_t)q * ldx];
-          u1 -= xi * Yt[p2 + (size_t)q * ldx];
-          v0 -= X[p1 + (size_t)q * ldx] * yi;
-          v1 -= X[p2 + (size_t)q * ldx] * yi;
+        {
+          // m is even: two independent FMA chains per output
+          double w0 = 0.0, w1 = 0.0, z0 = 0.0, z1 = 0.0;
+          const double *xi_ = X + i, *yi_ = Yt + i;
+          const double *xp1 = X + p1, *xp2 = X + p2, *yp1 = Yt + p1, *yp2 = Yt + p2;
+#pragma unroll 2
+          for (int q = 0; q < m; q += 2) {
+            const size_t o0 = (size_t)q * ldx, o1 = o0 + ldx;
+            const double xa = xi_[o0], ya = yi_[o0], xb = xi_[o1], yb = yi_[o1];
+            const double a1 = yp1[o0], a2 = yp2[o0], b1 = xp1[o0], b2 = xp2[o0];
+            const double c1 = yp1[o1], c2 = yp2[o1], d1 = xp1[o1], d2 = xp2[o1];
+            u0 -= xa * a1; u1 -= xa * a2; v0 -= b1 * ya; v1 -= b2 * ya;
+            w0 += xb * c1; w1 += xb * c2; z0 += d1 * yb; z1 += d2 * yb;
+          }
+          u0 -= w0; u1 -= w1; v0 -= z0; v1 -= z1;
         }
         // temp = Uhlp * Prodinv ; Vhlp = Delta (I - G)(P, :)
         X[i + (size_t)m * ldx] = u0 * q00 + u1 * q10;
