@@ -47,21 +47,38 @@ __device__ __noinline__ void blk_dmma(int m, int n, int k, double alpha, MatRef 
       for (int b = 0; b < 2; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
     const int ra0 = r0 + lr, ra1 = r0 + 8 + lr;
     const int cb0 = c0 + lr, cb1 = c0 + 8 + lr;
-    const bool full = plain && (r0 + 16 <= m) && (c0 + 16 <= n);
+    const bool full = (k & 3) == 0 && (r0 + 16 <= m) && (c0 + 16 <= n);
     if (full) {
       const double *pa0 = A.p + (size_t)ra0 * A.rs + (size_t)lc * A.cs;
       const double *pa1 = pa0 + (size_t)8 * A.rs;
       const double *pb0 = B.p + (size_t)lc * B.rs + (size_t)cb0 * B.cs;
       const double *pb1 = pb0 + (size_t)8 * B.cs;
       const size_t sa = (size_t)4 * A.cs, sb = (size_t)4 * B.rs;
+      if (plain) {
 #pragma unroll 4
-      for (int l0 = 0; l0 < k; l0 += 4) {
-        const double a0 = *pa0, a1 = *pa1, b0 = *pb0, b1 = *pb1;
-        pa0 += sa; pa1 += sa; pb0 += sb; pb1 += sb;
-        dmma884(acc[0][0][0], acc[0][0][1], a0, b0);
-        dmma884(acc[0][1][0], acc[0][1][1], a0, b1);
-        dmma884(acc[1][0][0], acc[1][0][1], a1, b0);
-        dmma884(acc[1][1][0], acc[1][1][1], a1, b1);
+        for (int l0 = 0; l0 < k; l0 += 4) {
+          const double a0 = *pa0, a1 = *pa1, b0 = *pb0, b1 = *pb1;
+          pa0 += sa; pa1 += sa; pb0 += sb; pb1 += sb;
+          dmma884(acc[0][0][0], acc[0][0][1], a0, b0);
+          dmma884(acc[0][1][0], acc[0][1][1], a0, b1);
+          dmma884(acc[1][0][0], acc[1][0][1], a1, b0);
+          dmma884(acc[1][1][0], acc[1][1][1], a1, b1);
+        }
+      } else {
+        // triangular operand: the same loop with the masked entries zeroed
+        // (no bounds checks inside a full tile)
+#pragma unroll 4
+        for (int l0 = 0; l0 < k; l0 += 4) {
+          const int l = l0 + lc;
+          double a0 = *pa0, a1 = *pa1, b0 = *pb0, b1 = *pb1;
+          pa0 += sa; pa1 += sa; pb0 += sb; pb1 += sb;
+          if (a_upper) { if (ra0 > l) a0 = 0.0; if (ra1 > l) a1 = 0.0; }
+          if (b_lower) { if (l < cb0) b0 = 0.0; if (l < cb1) b1 = 0.0; }
+          dmma884(acc[0][0][0], acc[0][0][1], a0, b0);
+          dmma884(acc[0][1][0], acc[0][1][1], a0, b1);
+          dmma884(acc[1][0][0], acc[1][0][1], a1, b0);
+          dmma884(acc[1][1][0], acc[1][1][1], a1, b1);
+        }
       }
     } else {
 #pragma unroll 4
