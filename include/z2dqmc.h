@@ -109,6 +109,15 @@ int z2_get_obs_equal(const z2_handle *h, int32_t chain, double out[Z2_NOBS_EQ]);
 /* out: Z2_NOBS_TAU arrays of (N, Ltrot) column-major, real parts (the
  * imaginary parts of ObserTau are identically zero for real G). */
 int z2_get_obs_tau(const z2_handle *h, int32_t chain, double *out);
+/* The same correlators in momentum space: Fourier_R_to_K (FFT_RtoK_2,
+ * src/lattice.f90:263-281) as applied by the reference's output layer
+ * (m_write_obs_tau, src/fourier_trans.f90:306-440),
+ *   gk(k, tau) = (1/N) sum_r exp(i k.r) g(r, tau),
+ * k = ((ix-1) 2pi/Nlx, (iy-1) 2pi/Nly) and r = (ix, iy) in the site order
+ * (x fastest), computed on the GPU.  re, im: [7][Ltrot][N] each, momentum
+ * index in place of the distance index of z2_get_obs_tau.  Needs a handle
+ * created with z2_options.tau = 1 (else Z2_ERR_STATE). */
+int z2_get_obs_tau_k(const z2_handle *h, int32_t chain, double *re, double *im);
 int z2_get_stats(const z2_handle *h, int32_t chain, double out[Z2_NSTATS]);
 /* Replay: use r[0..n) instead of ranf for the next n proposals (n = 0
  * restores ranf).  Decisions/ratios of the last half-sweeps, in the order

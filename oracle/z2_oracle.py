@@ -914,6 +914,46 @@ class ObserTau:
             np.add.at(a[name][:, nt], imj.ravel(), val.ravel())
 
 
+def k_dot_r(lat: Lattice) -> np.ndarray:
+    """Latt%k_dot_r (src/lattice.f90:159-173): xk_v(nk) = ((ix-1) 2pi/Nlx,
+    (iy-1) 2pi/Nly), aimj_v(imj) = (ix, iy) (1-based), k_dot_r(nk, imj)."""
+    xy = lat.n_list.astype(np.float64)
+    kx = (xy[:, 0] - 1.0) * 2.0 * np.pi / lat.Nlx
+    ky = (xy[:, 1] - 1.0) * 2.0 * np.pi / lat.Nly
+    return np.outer(kx, xy[:, 0]) + np.outer(ky, xy[:, 1])
+
+
+def fourier_r_to_k(gr: np.ndarray, lat: Lattice) -> np.ndarray:
+    """FFT_RtoK_2 (src/lattice.f90:263-281): gk(nk, nf) = sum_imj
+    exp(i k_dot_r(nk, imj)) gr(imj, nf) / Lq, summed in the reference's order
+    (imj outer, one term at a time)."""
+    kr = k_dot_r(lat)
+    ph = np.exp(1j * kr)
+    gk = np.zeros((lat.Lq, gr.shape[1]), dtype=np.complex128)
+    for imj in range(lat.Lq):
+        gk += ph[:, imj:imj + 1] * gr[imj:imj + 1, :]
+    return gk / float(lat.Lq)
+
+
+def integrate_susc(gk: np.ndarray, dtau: float) -> np.ndarray:
+    """m_integrate_susc_2_mom (src/fourier_trans.f90:165-177)."""
+    out = np.zeros(gk.shape[0], dtype=np.complex128)
+    for nt in range(gk.shape[1]):
+        out += gk[:, nt]
+    return out * dtau
+
+
+def integrate_susc_freq(gk: np.ndarray, dtau: float) -> np.ndarray:
+    """m_integrate_susc_2_freq (src/fourier_trans.f90:179-191): Matsubara
+    transform of the first momentum row."""
+    L = gk.shape[1]
+    out = np.zeros(L, dtype=np.complex128)
+    for nw in range(L):
+        for nt in range(L):
+            out[nw] += np.exp(1j * 2.0 * np.pi * nt * nw / L) * gk[0, nt]
+    return out * dtau
+
+
 # --------------------------------------------------------------------------
 # The model and the sweeps (src/localK.f90, src/local_sweep.f90,
 # src/dynamics.f90, src/multiply.f90)

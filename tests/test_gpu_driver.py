@@ -78,3 +78,36 @@ def test_driver_restart_from_confin(tmp_path):
     ref = _oracle_bins(p, [c])
     for k in ref:
         assert np.allclose(got[k], ref[k], rtol=1e-10, atol=1e-12), k
+
+
+def test_driver_tau_momentum_files(tmp_path):
+    """is_tau: the per-bin momentum-space files of m_write_obs_tau
+    (src/fourier_trans.f90:306-440), DFT on the GPU, against the oracle."""
+    build.build()
+    params = PARAMS.replace(".false. 0\n.false. 0\n.false. 0\n", ".true. 0\n.false. 0\n.false. 0\n")
+    (tmp_path / "paramC_sets.txt").write_text(params)
+    (tmp_path / "confin.txt").write_text("0\n")
+    (tmp_path / "seeds.txt").write_text("12345\n")
+    r = subprocess.run([build.DRIVER, "--chains", "1", "--dir", str(tmp_path)],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    p = zo.read_params(str(tmp_path / "paramC_sets.txt"))
+    assert p.is_tau
+    c = zo.Z2Chain(p, seed=12345)
+    c.pre()
+    lat = zo.Lattice(p.Nlx, p.Nly)
+    dtau = p.beta / p.Ltrot
+    want = {"sdw_zero_susc": [], "cdw_s_pipi_susc": [], "pair_d_zero_susc": [], "g_zero_susc": []}
+    src = {"sdw_zero_susc": ("spin", 0), "cdw_s_pipi_susc": ("charge_s", (p.Nly // 2) * p.Nlx + p.Nlx // 2),
+           "pair_d_zero_susc": ("pair_d", 0), "g_zero_susc": ("single", 0)}
+    for _ in range(p.Nbin):
+        c.sweep(toggle=True)
+        for f, (name, k) in src.items():
+            g = zo.integrate_susc(zo.fourier_r_to_k(c.obs_tau.arr[name], lat), dtau)
+            want[f].append(g[k])
+    for f, vals in want.items():
+        got = np.array([float(x) for x in (tmp_path / f).read_text().split()]).reshape(-1, 2)
+        ref = np.array([[v.real, v.imag] for v in vals])
+        assert np.allclose(got, ref, rtol=1e-9, atol=1e-12), f
+    for f in ("sdw_susc", "curxx_freq", "curxx_L_tau", "g_r0_tau", "pair_s_zero_tau"):
+        assert (tmp_path / f).stat().st_size > 0, f

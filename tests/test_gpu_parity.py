@@ -12,6 +12,7 @@ import pytest
 
 from oracle import z2_oracle as zo
 from z2_gauge_zfy_b200 import Chain, Z2Batch
+from z2_gauge_zfy_b200.api import integrate_susc, integrate_susc_freq
 
 pytestmark = pytest.mark.gpu
 RTOL = 1e-10
@@ -160,7 +161,7 @@ def _run_pair(ch, nbins=1, toggle=False, nsweep=1, replay=None, delay_k=0):
     rng = zo.ReplayStream(replay) if replay is not None else None
     c = zo.Z2Chain(p, seed=ch.seed, rng=rng, record_decisions=True)
     c.pre()
-    with Z2Batch([ch], record=True, delay_k=delay_k) as b:
+    with Z2Batch([ch], record=True, delay_k=delay_k, tau=toggle) as b:
         if replay is not None:
             b.set_replay(0, replay)
         b.pre()
@@ -170,7 +171,8 @@ def _run_pair(ch, nbins=1, toggle=False, nsweep=1, replay=None, delay_k=0):
             c.sweep(toggle=toggle, nsweep=nsweep)
             b.sweep(nsweep, toggle)
             res.append((b.green(0), b.obs_equal(0), b.stats(0), b.decisions(0),
-                        b.obs_tau(0) if toggle else None, b.get_config(0)))
+                        b.obs_tau(0) if toggle else None, b.get_config(0),
+                        b.obs_tau_k(0) if toggle else None))
     return c, res
 
 
@@ -186,7 +188,7 @@ def _decisions_oracle(c, L, nb):
 def test_sweep_parity_c1():
     ch = C1
     c, res = _run_pair(ch, nbins=2)
-    G, obs, st, (dec, rat), _, (sig, iseed) = res[-1]
+    G, obs, st, (dec, rat), _, (sig, iseed), _ = res[-1]
     dec_o, rat_o = _decisions_oracle(c, ch.Ltrot, 2 * ch.N)
     assert np.array_equal(dec, dec_o)
     assert rel(rat, rat_o) < RTOL
@@ -205,7 +207,7 @@ def test_sweep_parity_mu_replay_all_accept():
                seed=99)
     n = 2 * 2 * ch.N * ch.Ltrot
     c, res = _run_pair(ch, replay=np.zeros(n))
-    G, obs, st, (dec, rat), _, (sig, _) = res[-1]
+    G, obs, st, (dec, rat), _, (sig, _), _ = res[-1]
     dec_o, rat_o = _decisions_oracle(c, ch.Ltrot, 2 * ch.N)
     assert np.array_equal(dec, dec_o)
     assert rel(G, c.prop.Gr) < RTOL
@@ -216,11 +218,22 @@ def test_sweep_parity_tau():
     ch = Chain(RT=1.0, J=0.5, h=0.5, mu=0.1, Nlx=4, Nly=4, Ltrot=20, beta=2.0, Nwrap=5,
                seed=2024)
     c, res = _run_pair(ch, toggle=True)
-    G, obs, st, _, otau, _ = res[-1]
+    G, obs, st, _, otau, _, otau_k = res[-1]
     assert rel(G, c.prop.Gr) < RTOL
+    lat = zo.Lattice(ch.Nlx, ch.Nly)
+    dtau = ch.beta / ch.Ltrot
     for q, k in enumerate(zo.TAU_NAMES):
         ref = np.real(c.obs_tau.arr[k])
         assert rel(otau[k], ref) < 1e-9, k
+        # momentum space (Fourier_R_to_K of the output layer) on the GPU
+        gk_ref = zo.fourier_r_to_k(c.obs_tau.arr[k], lat)
+        assert np.max(np.abs(otau_k[k] - gk_ref)) <= 1e-9 * max(np.max(np.abs(gk_ref)), 1e-12), k
+        s_ref = zo.integrate_susc(gk_ref, dtau)
+        assert np.max(np.abs(integrate_susc(otau_k[k], dtau) - s_ref)) <= \
+            1e-9 * max(np.max(np.abs(s_ref)), 1e-12), k
+    w_ref = zo.integrate_susc_freq(zo.fourier_r_to_k(c.obs_tau.arr["curxx"], lat), dtau)
+    w = integrate_susc_freq(otau_k["curxx"], dtau)
+    assert np.max(np.abs(w - w_ref)) <= 1e-9 * max(np.max(np.abs(w_ref)), 1e-12)
 
 
 def test_logdet_grad_parity():
@@ -247,7 +260,7 @@ def test_sweep_parity_L16_global_G():
     ch = Chain(RT=1.0, J=0.5, h=0.6, mu=0.0, Nlx=16, Nly=16, Ltrot=16, beta=0.8, Nwrap=8,
                seed=4321)
     c, res = _run_pair(ch)
-    G, obs, st, (dec, rat), _, (sig, iseed) = res[-1]
+    G, obs, st, (dec, rat), _, (sig, iseed), _ = res[-1]
     dec_o, _ = _decisions_oracle(c, ch.Ltrot, 2 * ch.N)
     assert np.array_equal(dec, dec_o)
     assert np.array_equal(sig, c.sigma) and iseed == c.rng.state

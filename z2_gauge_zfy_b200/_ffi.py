@@ -28,7 +28,7 @@ EXPORTS = (
     "z2_get_obs_equal", "z2_get_obs_tau", "z2_get_stats", "z2_set_replay",
     "z2_get_decisions", "z2_logdet_grad", "z2_opk_mmult_R", "z2_opk_mmult_L",
     "z2_stab_UR", "z2_stab_UL", "z2_stab_green", "z2_stab_green_big",
-    "z2_stab_green_noalloc", "z2_get_phase_cycles", "z2_tune_delay",
+    "z2_stab_green_noalloc", "z2_get_phase_cycles", "z2_tune_delay", "z2_get_obs_tau_k",
 )
 Z2_NOALLOC_NMAX = 144
 
@@ -83,6 +83,7 @@ def load():
         "z2_get_green": (C.c_int, [vp, i32, dp]),
         "z2_get_obs_equal": (C.c_int, [vp, i32, dp]),
         "z2_get_obs_tau": (C.c_int, [vp, i32, dp]),
+        "z2_get_obs_tau_k": (C.c_int, [vp, i32, dp, dp]),
         "z2_get_stats": (C.c_int, [vp, i32, dp]),
         "z2_set_replay": (C.c_int, [vp, i32, dp, C.c_size_t]),
         "z2_get_decisions": (C.c_int, [vp, i32, C.POINTER(C.c_uint8), dp, C.c_size_t]),

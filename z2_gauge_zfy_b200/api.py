@@ -62,6 +62,22 @@ def _check(lib, h, code):
         raise Z2Error(code, msg.decode() if msg else "")
 
 
+def integrate_susc(gk: np.ndarray, dtau: float) -> np.ndarray:
+    """Static susceptibility per momentum, dtau * sum_tau gk(k, tau)
+    (m_integrate_susc_2_mom, src/fourier_trans.f90:165-177)."""
+    return gk.sum(axis=1) * dtau
+
+
+def integrate_susc_freq(gk: np.ndarray, dtau: float) -> np.ndarray:
+    """Matsubara transform of the k = 0 row, dtau * sum_tau
+    exp(2 pi i (tau-1)(w-1)/Ltrot) gk(0, tau), w = 1..Ltrot
+    (m_integrate_susc_2_freq, src/fourier_trans.f90:179-191)."""
+    L = gk.shape[1]
+    t = np.arange(L)
+    ph = np.exp(2j * np.pi * np.outer(t, t) / L)
+    return (ph @ gk[0]) * dtau
+
+
 def _params(chains):
     """ctypes array of z2_chain_params (and the per-bond arrays it points to)."""
     n = len(chains)
@@ -202,6 +218,17 @@ class Z2Batch:
         buf = np.empty(7 * N * L)
         self._c(self.lib.z2_get_obs_tau(self.h, chain, dptr(buf)))
         a = buf.reshape(7, L, N)
+        return {k: a[q].T.copy() for q, k in enumerate(OBS_TAU_NAMES)}
+
+    def obs_tau_k(self, chain: int) -> dict:
+        """Time-displaced correlators in momentum space (``z2_get_obs_tau_k``,
+        Fourier_R_to_K of the reference's output layer): name -> complex
+        array [N (momentum index), Ltrot]."""
+        N, L, _ = self.dims(chain)
+        re = np.empty(7 * N * L)
+        im = np.empty(7 * N * L)
+        self._c(self.lib.z2_get_obs_tau_k(self.h, chain, dptr(re), dptr(im)))
+        a = (re + 1j * im).reshape(7, L, N)
         return {k: a[q].T.copy() for q, k in enumerate(OBS_TAU_NAMES)}
 
     def stats(self, chain: int) -> dict:

@@ -197,6 +197,8 @@ struct ChainHost {
   size_t bytes = 0;
   char *base = nullptr;              // device allocation of this chain
   double *replay = nullptr;
+  double *ktab = nullptr;            // [2][N][N] cos, sin of k.r (tau chains only)
+  double *kout = nullptr;            // [2][7][Ltrot][N] k-space correlators
 };
 
 }  // namespace
@@ -467,6 +469,8 @@ extern "C" int z2_create(z2_handle **out, const z2_chain_params *params, int32_t
     size_t o_grad = take(8 * (size_t)nb);
     size_t o_acc = take(8 * A_COUNT);
     size_t o_misc = take(64);                     // rng, replay_pos, status
+    size_t o_ktab = 0, o_kout = 0;
+    if (h->opt.tau) { o_ktab = take(8 * NN * 2); o_kout = take(8 * (size_t)14 * Lt * N); }
     size_t o_dec = 0, o_rat = 0;
     if (h->opt.record) { o_dec = take((size_t)2 * Lt * nb); o_rat = take(8 * (size_t)2 * Lt * nb); }
     C.bytes = off;
@@ -489,6 +493,23 @@ extern "C" int z2_create(z2_handle **out, const z2_chain_params *params, int32_t
     CUDA_TRY(h, up(o_stag, stag.data(), 8 * stag.size()));
     CUDA_TRY(h, up(o_psh, psh.data(), 8 * psh.size()));
     CUDA_TRY(h, up(o_sigma, C.sigma0.data(), C.sigma0.size()));
+    if (h->opt.tau) {
+      // exp(i k.r) of Fourier_R_to_K (src/lattice.f90:159-173, 263-281):
+      // k = ((ix-1) 2pi/Nlx, (iy-1) 2pi/Nly), r = (ix, iy) 1-based
+      std::vector<double> kt(2 * NN);
+      const double PI2 = 2.0 * std::acos(-1.0);
+      for (int r = 0; r < N; ++r)
+        for (int k = 0; k < N; ++k) {
+          const double kx = (double)(lat.xy[2 * k] - 1) * PI2 / (double)p.Nlx;
+          const double ky = (double)(lat.xy[2 * k + 1] - 1) * PI2 / (double)p.Nly;
+          const double kr = kx * (double)lat.xy[2 * r] + ky * (double)lat.xy[2 * r + 1];
+          kt[k + (size_t)r * N] = std::cos(kr);
+          kt[NN + k + (size_t)r * N] = std::sin(kr);
+        }
+      CUDA_TRY(h, up(o_ktab, kt.data(), 8 * kt.size()));
+      C.ktab = (double *)(base + o_ktab);
+      C.kout = (double *)(base + o_kout);
+    }
     ChainDesc &d = C.d;
     d.beta = p.beta; d.dtau = C.dtau;
     d.eP = std::exp(C.dtau * p.mu); d.eM = std::exp(-C.dtau * p.mu);
@@ -728,6 +749,42 @@ extern "C" int z2_get_obs_tau(const z2_handle *h, int32_t chain, double *out) {
   CUDA_TRY(hh, cudaSetDevice(h->device));
   CUDA_TRY(hh, cudaMemcpy(out, C.d.obs_tau, sizeof(double) * 7 * C.Ltrot * C.N,
                           cudaMemcpyDeviceToHost));
+  return Z2_OK;
+}
+
+// Fourier_R_to_K of the seven time-displaced correlators of one chain
+// (FFT_RtoK_2, src/lattice.f90:263-281, as called by m_write_obs_tau,
+// src/fourier_trans.f90:306-440): out = exp(i k.r) [N x N] times the
+// correlators [N x 7 Ltrot] / N, as two DMMA GEMMs (cos and sin parts; the
+// correlators are real).  One CTA per slab of 64 columns.
+__global__ void __launch_bounds__(Z2_NT, 1)
+z2_kspace_kernel(int N, int ncol, const double *tab, const double *obs, double *out) {
+  const int c0 = blockIdx.x * 64;
+  const int nc = (ncol - c0) < 64 ? (ncol - c0) : 64;
+  if (nc <= 0) return;
+  const double sc = 1.0 / (double)N;
+  for (int part = 0; part < 2; ++part)
+    blk_dmma(N, nc, N, sc, MatRef{tab + (size_t)part * N * N, 1, N}, false,
+             MatRef{obs + (size_t)c0 * N, 1, N}, false, 0.0,
+             out + (size_t)part * N * ncol + (size_t)c0 * N, N);
+}
+
+extern "C" int z2_get_obs_tau_k(const z2_handle *h, int32_t chain, double *re, double *im) {
+  int r = check_chain(h, chain);
+  if (r) return r;
+  z2_handle *hh = const_cast<z2_handle *>(h);
+  if (!re || !im) return set_err(hh, Z2_ERR_ARG, "z2_get_obs_tau_k: null output");
+  const ChainHost &C = h->ch[chain];
+  if (!C.ktab)
+    return set_err(hh, Z2_ERR_STATE, "z2_get_obs_tau_k: handle created without tau (z2_options.tau)");
+  CUDA_TRY(hh, cudaSetDevice(h->device));
+  const int ncol = 7 * C.Ltrot;
+  z2_kspace_kernel<<<(ncol + 63) / 64, Z2_NT, 0, h->stream>>>(C.N, ncol, C.ktab, C.d.obs_tau, C.kout);
+  CUDA_TRY(hh, cudaGetLastError());
+  const size_t n = (size_t)ncol * C.N;
+  CUDA_TRY(hh, cudaMemcpyAsync(re, C.kout, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(hh, cudaMemcpyAsync(im, C.kout + n, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(hh, cudaStreamSynchronize(h->stream));
   return Z2_OK;
 }
 

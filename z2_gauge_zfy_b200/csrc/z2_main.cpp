@@ -18,6 +18,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdint>
+#include <complex>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -199,6 +200,134 @@ void append(const std::string &dir, const char *name, double v) {
   std::fclose(f);
 }
 
+// ---------------------------------------------------------------------------
+// Momentum-space output of the time-displaced correlators, one record per bin
+// in the files of m_write_obs_tau (src/fourier_trans.f90:306-440).  The DFT
+// (Fourier_R_to_K) runs on the GPU (z2_get_obs_tau_k, averaged over chains);
+// the tau integration and the Matsubara transform of curxx are O(N Ltrot) and
+// O(Ltrot^2) host loops.  Numbers are written with %.17g (the reference uses
+// Fortran list-directed output: same values, different spacing).
+// ---------------------------------------------------------------------------
+struct KOut {
+  const std::string &dir;
+  int N, Lt, Nlx, Nly;
+  double dtau, beta;
+  void k_line(FILE *f, int k) const {   // Latt%xk_v(k, 1:2)
+    const double PI2 = 2.0 * std::acos(-1.0);
+    std::fprintf(f, " %.17g %.17g\n", (double)(k % Nlx) * PI2 / Nlx, (double)(k / Nlx) * PI2 / Nly);
+  }
+  FILE *open(const char *name) const { return std::fopen((dir + "/" + name).c_str(), "a"); }
+  // write_reciprocal_1: per k the momentum, then gk
+  void reciprocal(const char *name, const std::vector<std::complex<double>> &g) const {
+    FILE *f = open(name); if (!f) return;
+    for (int k = 0; k < N; ++k) { k_line(f, k); std::fprintf(f, " (%.17g,%.17g)\n", g[k].real(), g[k].imag()); }
+    std::fclose(f);
+  }
+  // write_k_1: one momentum
+  void at_k(const char *name, const std::vector<std::complex<double>> &g, int k) const {
+    FILE *f = open(name); if (!f) return;
+    std::fprintf(f, " %.17g %.17g\n", g[k].real(), g[k].imag());
+    std::fclose(f);
+  }
+  // write_k_tau_2: momentum, then gk(k, tau) for every tau
+  void k_tau(const char *name, const double *re, const double *im, int k) const {
+    FILE *f = open(name); if (!f) return;
+    k_line(f, k);
+    for (int t = 0; t < Lt; ++t) std::fprintf(f, " %.17g %.17g\n", re[(size_t)t * N + k], im[(size_t)t * N + k]);
+    std::fclose(f);
+  }
+  // integrate_susc: dtau * sum_tau gk(k, tau)
+  std::vector<std::complex<double>> susc(const double *re, const double *im) const {
+    std::vector<std::complex<double>> g(N, 0.0);
+    for (int t = 0; t < Lt; ++t)
+      for (int k = 0; k < N; ++k) g[k] += std::complex<double>(re[(size_t)t * N + k], im[(size_t)t * N + k]);
+    for (auto &x : g) x *= dtau;
+    return g;
+  }
+};
+
+static void write_obs_tau_k(z2_handle *h, const std::string &dir, const Params &p, int nch,
+                            const std::vector<double> &tau_real) {
+  const int N = p.Nlx * p.Nly, Lt = p.Ltrot;
+  const size_t n = (size_t)7 * Lt * N;
+  std::vector<double> re(n), im(n), sr(n, 0.0), si(n, 0.0);
+  for (int c = 0; c < nch; ++c) {
+    if (z2_get_obs_tau_k(h, c, re.data(), im.data())) return;
+    for (size_t i = 0; i < n; ++i) { sr[i] += re[i] / nch; si[i] += im[i] / nch; }
+  }
+  const KOut o{dir, N, Lt, p.Nlx, p.Nly, p.beta / Lt, p.beta};
+  const bool has_pi = (p.Nlx % 2 == 0) && (p.Nly % 2 == 0);
+  const int kzero = 0, kpi = (p.Nly / 2) * p.Nlx + p.Nlx / 2;
+  const int kqx = p.Nlx > 1 ? 1 : kzero, kqy = p.Nly > 1 ? p.Nlx : kzero;
+  auto R = [&](int q) { return sr.data() + (size_t)q * Lt * N; };
+  auto I = [&](int q) { return si.data() + (size_t)q * Lt * N; };
+  // correlator order: spin, single, pair_d, pair_s, charge_d, charge_s, curxx
+  {
+    auto g = o.susc(R(0), I(0));
+    o.reciprocal("sdw_susc", g);
+    if (has_pi) o.at_k("sdw_pipi_susc", g, kpi);
+    o.at_k("sdw_zero_susc", g, kzero);
+  }
+  const char *cd[2][5] = {{"cdw_d_pipi_tau", "cdw_d_susc", "cdw_d_pipi_susc", "cdw_d_zero_susc", ""},
+                          {"cdw_s_pipi_tau", "cdw_s_susc", "cdw_s_pipi_susc", "cdw_s_zero_susc", ""}};
+  for (int w = 0; w < 2; ++w) {
+    const int q = 4 + w;
+    if (has_pi) o.k_tau(cd[w][0], R(q), I(q), kpi);
+    auto g = o.susc(R(q), I(q));
+    o.reciprocal(cd[w][1], g);
+    if (has_pi) o.at_k(cd[w][2], g, kpi);
+    o.at_k(cd[w][3], g, kzero);
+  }
+  {
+    // g_r0_tau: real-space single-particle correlator at imj = Lq, / Lq
+    FILE *f = o.open("g_r0_tau");
+    if (f) {
+      std::fprintf(f, " %d %d\n", p.Nlx, p.Nly);   // Latt%aimj_v(Lq, 1:2)
+      const double *g1 = tau_real.data() + (size_t)1 * Lt * N;
+      for (int t = 0; t < Lt; ++t) std::fprintf(f, " %.17g %.17g\n", g1[(size_t)t * N + N - 1] / N, 0.0);
+      std::fclose(f);
+    }
+    auto g = o.susc(R(1), I(1));
+    o.reciprocal("g_susc", g);
+    if (has_pi) o.at_k("g_pipi_susc", g, kpi);
+    o.at_k("g_zero_susc", g, kzero);
+  }
+  {
+    const int q = 6;
+    if (p.Nlx > 1) o.k_tau("curxx_L_tau", R(q), I(q), kqx);
+    if (p.Nly > 1) o.k_tau("curxx_T_tau", R(q), I(q), kqy);
+    o.k_tau("curxx_zero_tau", R(q), I(q), kzero);
+    auto g = o.susc(R(q), I(q));
+    // Matsubara transform of the k = 0 row (integrate_susc_freq)
+    FILE *f = o.open("curxx_freq");
+    if (f) {
+      const double PI2 = 2.0 * std::acos(-1.0);
+      for (int w = 0; w < Lt; ++w) {
+        std::complex<double> s(0.0, 0.0);
+        for (int t = 0; t < Lt; ++t)
+          s += std::exp(std::complex<double>(0.0, PI2 * (double)t * (double)w / Lt)) *
+               std::complex<double>(R(q)[(size_t)t * N], I(q)[(size_t)t * N]);
+        s *= o.dtau;
+        std::fprintf(f, " %.17g\n %.17g %.17g\n", PI2 * w / p.beta, s.real(), s.imag());
+      }
+      std::fclose(f);
+    }
+    o.reciprocal("curxx_susc", g);
+    if (p.Nlx > 1) o.at_k("curxx_L_susc", g, kqx);
+    if (p.Nly > 1) o.at_k("curxx_T_susc", g, kqy);
+    o.at_k("curxx_zero_susc", g, kzero);
+  }
+  const char *pr[2][3] = {{"pair_s_zero_tau", "pair_s_susc", "pair_s_zero_susc"},
+                          {"pair_d_zero_tau", "pair_d_susc", "pair_d_zero_susc"}};
+  for (int w = 0; w < 2; ++w) {
+    const int q = w == 0 ? 3 : 2;
+    o.k_tau(pr[w][0], R(q), I(q), kzero);
+    auto g = o.susc(R(q), I(q));
+    o.reciprocal(pr[w][1], g);
+    o.at_k(pr[w][2], g, kzero);
+  }
+}
+
 int fail(z2_handle *h, const char *what, int code) {
   std::fprintf(stderr, "%s failed (%d): %s\n", what, code, h ? z2_last_error(h) : "");
   return 1;
@@ -311,6 +440,7 @@ int main(int argc, char **argv) {
       }
       FILE *f = std::fopen((dir + "/obs_tau_raw").c_str(), "a");
       if (f) { for (double v : tau_sum) std::fprintf(f, " %25.17E\n", v); std::fclose(f); }
+      write_obs_tau_k(h, dir, p, nch, tau_sum);
     }
     if (nbc % 20 == 0 && info) {
       double acc = 0;
