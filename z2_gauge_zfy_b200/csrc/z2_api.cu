@@ -103,7 +103,7 @@ namespace {
 const double kZero = 1.0e-10;      // src/calc_basic.f90:5
 const double kUpbound = 1.0e200;   // src/calc_basic.f90:7
 const int kSmemMax = 227 * 1024 - 2048;
-const int kGemmTile = 2 * Z2_GEMM_TK * (Z2_GEMM_TM + 1);
+const int kGemmTile = Z2_MIN_TILE;
 
 int npbc(int nr, int L) { return nr < 1 ? nr + L : (nr > L ? nr - L : nr); }
 

@@ -198,7 +198,8 @@ __device__ __noinline__ void apply_pending_L(const ChainDesc &c, const Smem &s, 
 // stab_green_big (src/stabilization.f90:202-264): the four blocks of the
 // 2N x 2N Green's function.  Inverses of the orthogonal factors (UL UR,
 // bigU, UR, UL) are their transposes; VR VL, VR and VL are inverted by LU;
-// bigV (triangular) by a triangular solve.
+// bigV (triangular) by a triangular solve.  The 2N x 2N QR (UDV_C) is the
+// blocked Householder QR, bigU the blocked DORGQR, products DMMA GEMMs.
 __device__ __noinline__ void dev_stab_green_big(const Smem &s, int N, const double *UR, const double *DR,
                                    const double *VR, const double *ULT, const double *DL,
                                    const double *VL, double *W0, double *W1, double *W2,
@@ -209,14 +210,12 @@ __device__ __noinline__ void dev_stab_green_big(const Smem &s, int N, const doub
   int *ipiv = s.ivec;
   // invVRVL = (VR VL)^-1  -> W0
   {
-    GemmOp op{VR, N, false, false, VL, N, false, false};
-    blk_gemm(N, N, N, 1.0, op, 0.0, W0, N, s.tile);
+    blk_dmma(N, N, N, 1.0, MatRef{VR, 1, N}, false, MatRef{VL, 1, N}, false, 0.0, W0, N);
     blk_inverse(W0, N, N, W1, N, ipiv, s.red, s.flag);
   }
   // invULUR = UR^T UL^T -> W1
   {
-    GemmOp op{UR, N, true, false, ULT, N, false, false};
-    blk_gemm(N, N, N, 1.0, op, 0.0, W1, N, s.tile);
+    blk_dmma(N, N, N, 1.0, MatRef{UR, N, 1}, false, MatRef{ULT, 1, N}, false, 0.0, W1, N);
   }
   // big matrix
   for (int j = threadIdx.x / 32; j < n2; j += Z2_WARPS)
@@ -230,9 +229,9 @@ __device__ __noinline__ void dev_stab_green_big(const Smem &s, int N, const doub
     }
   __syncthreads();
   // UDV_C: QR, D = |R_ii|, V = R / D, determinant-sign fix
-  blk_geqr2(B0, n2, n2, n2, tau);
+  blk_geqrf(B0, n2, n2, tau, s.tile, s.tile_doubles, s.vec + 4 * N, 4 * N, s.red);
   blk_copy(B1, n2, B0, n2, n2, n2);
-  blk_org2r(B1, n2, n2, n2, tau);                 // bigU
+  blk_orgqr(B1, n2, n2, tau, s.tile, s.tile_doubles, s.vec + 4 * N, 4 * N);   // bigU
   {
     // sign of prod R_ii (mat_mod.f90:650-657): count negative diagonals
     int neg = 0;
@@ -254,7 +253,7 @@ __device__ __noinline__ void dev_stab_green_big(const Smem &s, int N, const doub
   }
   // invbigV: solve bigV X = I -> B3
   blk_identity(B3, n2, n2);
-  blk_trsm_LUN(B2, n2, n2, B3, n2, n2);
+  blk_trsm_lun_blocked(B2, n2, n2, B3, n2, n2);
   // invVUR -> W2, invVUL -> W3
   blk_copy(W2, N, VR, N, N, N);
   blk_inverse(W2, N, N, W0, N, ipiv, s.red, s.flag);
@@ -262,17 +261,14 @@ __device__ __noinline__ void dev_stab_green_big(const Smem &s, int N, const doub
   blk_inverse(W3, N, N, W0, N, ipiv, s.red, s.flag);
   // mat_left = diag(invVUR, invUUL) invbigV -> B0
   {
-    GemmOp op{W2, N, false, false, B3, n2, false, false};
-    blk_gemm(N, n2, N, 1.0, op, 0.0, B0, n2, s.tile);
-    GemmOp op2{ULT, N, false, false, B3 + N, n2, false, false};
-    blk_gemm(N, n2, N, 1.0, op2, 0.0, B0 + N, n2, s.tile);
+    blk_dmma(N, n2, N, 1.0, MatRef{W2, 1, N}, false, MatRef{B3, 1, n2}, false, 0.0, B0, n2);
+    blk_dmma(N, n2, N, 1.0, MatRef{ULT, 1, N}, false, MatRef{B3 + N, 1, n2}, false, 0.0, B0 + N, n2);
   }
   // mat_right = invbigU diag(invVUL, invUUR) -> B2 ; invbigU = bigU^T
   {
-    GemmOp op{B1, n2, true, false, W3, N, false, false};
-    blk_gemm(n2, N, N, 1.0, op, 0.0, B2, n2, s.tile);
-    GemmOp op2{B1 + N, n2, true, false, UR, N, true, false};
-    blk_gemm(n2, N, N, 1.0, op2, 0.0, B2 + (size_t)N * n2, n2, s.tile);
+    blk_dmma(n2, N, N, 1.0, MatRef{B1, n2, 1}, false, MatRef{W3, 1, N}, false, 0.0, B2, n2);
+    blk_dmma(n2, N, N, 1.0, MatRef{B1 + N, n2, 1}, false, MatRef{UR, N, 1}, false, 0.0,
+             B2 + (size_t)N * n2, n2);
   }
   // mat_left(:, nr) /= bigD(nr)
   for (int j = threadIdx.x / 32; j < n2; j += Z2_WARPS) {
@@ -281,8 +277,7 @@ __device__ __noinline__ void dev_stab_green_big(const Smem &s, int N, const doub
   }
   __syncthreads();
   {
-    GemmOp op{B0, n2, false, false, B2, n2, false, false};
-    blk_gemm(n2, n2, n2, 1.0, op, 0.0, B3, n2, s.tile);
+    blk_dmma(n2, n2, n2, 1.0, MatRef{B0, 1, n2}, false, MatRef{B2, 1, n2}, false, 0.0, B3, n2);
   }
 }
 

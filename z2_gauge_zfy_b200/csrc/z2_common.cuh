@@ -12,9 +12,7 @@
 #define Z2_WARPS (Z2_NT / 32)
 #define Z2_FULL 0xffffffffu
 #define Z2_NRED 64              // doubles of block-reduction scratch
-#define Z2_GEMM_TM 64           // tiled GEMM: C tile rows
-#define Z2_GEMM_TN 64           // C tile cols
-#define Z2_GEMM_TK 16           // K chunk
+#define Z2_MIN_TILE 2080        // doubles of shared work space kept after G and X, Y
 
 // Accumulator layout of ChainDesc::acc (doubles).
 enum {

@@ -368,6 +368,127 @@ __device__ __noinline__ void blk_orgqr(double *A, int lda, int n, const double *
   }
 }
 
+// Householder QR without pivoting of a square n x n matrix, blocked (DGEQRF
+// structure): panels of nb columns are factored column by column (DLARFG on
+// the column, the reflector applied to the rest of the panel one warp per
+// column), then the panel's reflectors reach the trailing columns as
+// C <- (I - V T^T V^T) C = C - V (T^T (V^T C)) by DMMA GEMMs (T by DLARFT's
+// recurrence, as in blk_orgqr).  Same R, tau and reflectors as DGEQR2 up to
+// rounding.  Workspace as blk_orgqr; falls back to blk_geqr2 when short.
+__device__ __noinline__ void blk_geqrf(double *A, int lda, int n, double *tau, double *work, int wd,
+                                      double *small, int sd, double *red) {
+  const int ldv = ((n + 11) & ~15) + 4;
+  int nb = 16;
+  auto need = [n, ldv, sd](int b) {
+    return ldv * b + (b + 1) * (n > b ? n - b : 0) + (2 * b * b <= sd ? 0 : 2 * b * b);
+  };
+  if (need(nb) > wd) nb = 8;
+  if (need(nb) > wd) {
+    blk_geqr2(A, lda, n, n, tau);
+    return;
+  }
+  const int ldw = nb + 1;
+  double *V = work;
+  double *W = V + (size_t)ldv * nb;
+  double *T = (2 * nb * nb <= sd) ? small : W + (size_t)ldw * (n > nb ? n - nb : 0);
+  double *S = T + nb * nb;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int j0 = 0; j0 < n; j0 += nb) {
+    const int ib = (n - j0) < nb ? (n - j0) : nb;
+    const int mp = n - j0, nc = n - j0 - ib;
+    // ---- panel (DGEQR2 on columns j0 .. j0+ib-1) ----
+    for (int k = 0; k < ib; ++k) {
+      const int j = j0 + k;
+      double *Aj = A + (size_t)j * lda;
+      double ss = 0.0;
+      for (int r = j + 1 + tid; r < n; r += Z2_NT) { const double a = Aj[r]; ss += a * a; }
+      ss = blk_sum(ss, red);
+      const double alpha = Aj[j];
+      double t = 0.0, beta = alpha, sc = 1.0;
+      if (j < n - 1 && ss != 0.0) {
+        const double xnorm = sqrt(ss);
+        beta = -copysign(dlapy2(alpha, xnorm), alpha);
+        t = (beta - alpha) / beta;
+        sc = 1.0 / (alpha - beta);
+      }
+      if (t != 0.0)
+        for (int r = j + 1 + tid; r < n; r += Z2_NT) Aj[r] *= sc;
+      __syncthreads();
+      // H_j on the remaining panel columns, one warp per column (v_j = 1)
+      if (t != 0.0) {
+        for (int c = j + 1 + warp; c < j0 + ib; c += Z2_WARPS) {
+          double *Ac = A + (size_t)c * lda;
+          const double acj = Ac[j];
+          double w = 0.0;
+          for (int r = j + 1 + lane; r < n; r += 32) w += Aj[r] * Ac[r];
+          w = (warp_sum(w) + acj) * t;
+          __syncwarp();
+          if (lane == 0) Ac[j] = acj - w;
+          for (int r = j + 1 + lane; r < n; r += 32) Ac[r] -= w * Aj[r];
+        }
+      }
+      __syncthreads();
+      if (tid == 0) { tau[j] = t; Aj[j] = beta; }
+      __syncthreads();
+    }
+    if (nc <= 0) continue;
+    // ---- V (unit lower), S = V^T V, T (DLARFT) ----
+    for (int e = tid; e < mp * ib; e += Z2_NT) {
+      const int r = e % mp, c = e / mp;
+      V[r + (size_t)c * ldv] = (r == c) ? 1.0 : (r > c ? A[(j0 + r) + (size_t)(j0 + c) * lda] : 0.0);
+    }
+    __syncthreads();
+    blk_dmma(ib, ib, mp, 1.0, MatRef{V, ldv, 1}, false, MatRef{V, 1, ldv}, false, 0.0, S, ib);
+    if (tid < ib) {
+      const int r = tid;
+      double tr[16];
+#pragma unroll
+      for (int c = 0; c < 16; ++c) {
+        double t = 0.0;
+        if (c < ib) {
+          if (c == r) {
+            t = tau[j0 + c];
+          } else if (c > r) {
+            double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+            for (int q = 0; q < c; ++q) {
+              if (q >= r) {
+                if (q & 1) a1 += tr[q] * S[q + c * ib];
+                else a0 += tr[q] * S[q + c * ib];
+              }
+            }
+            t = -tau[j0 + c] * (a0 + a1);
+          }
+        }
+        tr[c] = t;
+      }
+#pragma unroll
+      for (int c = 0; c < 16; ++c)
+        if (c < ib) T[r + c * ib] = tr[c];
+    }
+    __syncthreads();
+    // ---- trailing columns: C -= V (T^T (V^T C)) ----
+    double *C = A + j0 + (size_t)(j0 + ib) * lda;
+    blk_dmma(ib, nc, mp, 1.0, MatRef{V, ldv, 1}, false, MatRef{C, 1, lda}, false, 0.0, W, ldw);
+    for (int c = tid; c < nc; c += Z2_NT) {
+      double w[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) w[q] = (q < ib) ? W[q + c * ldw] : 0.0;
+#pragma unroll
+      for (int r = 0; r < 16; ++r) {
+        if (r < ib) {
+          double t = 0.0;
+#pragma unroll
+          for (int q = 0; q <= r; ++q) t += T[q + r * ib] * w[q];   // (T^T w)_r
+          W[r + c * ldw] = t;
+        }
+      }
+    }
+    __syncthreads();
+    blk_dmma(mp, nc, ib, -1.0, MatRef{V, 1, ldv}, false, MatRef{W, 1, ldw}, false, 1.0, C, lda);
+  }
+}
+
 // Solve R Z = Y in place (DTRSM 'L','U','N','N'), Y n x nc (ldy), R upper
 // (ldr).  Blocks of 8 rows from the bottom: the 8 x 8 diagonal block is
 // solved one thread per column (block of R held in registers), the rows

@@ -223,121 +223,6 @@ __device__ __noinline__ void blk_qdrp_scale(double *A, int lda, int n, double *D
   __syncthreads();
 }
 
-// DORG2R: form Q (m x n, m >= n) in place from n reflectors.
-__device__ __noinline__ void blk_org2r(double *A, int lda, int m, int n, const double *tau) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int i = n - 1; i >= 0; --i) {
-    const double ti = tau[i];
-    if (i < n - 1 && ti != 0.0) {
-      const double *v = A + (size_t)i * lda;
-      for (int k = i + 1 + warp; k < n; k += Z2_WARPS) {
-        double *Ak = A + (size_t)k * lda;
-        double w = 0.0;
-        for (int r = i + 1 + lane; r < m; r += 32) w += v[r] * Ak[r];
-        w = warp_sum(w) + Ak[i];
-        double tw = ti * w;
-        __syncwarp();
-        if (lane == 0) Ak[i] -= tw;
-        for (int r = i + 1 + lane; r < m; r += 32) Ak[r] -= v[r] * tw;
-      }
-    }
-    __syncthreads();
-    double *Ai = A + (size_t)i * lda;
-    for (int r = threadIdx.x; r < m; r += Z2_NT) {
-      if (r > i) Ai[r] *= -ti;
-      else if (r == i) Ai[r] = 1.0 - ti;
-      else Ai[r] = 0.0;
-    }
-    __syncthreads();
-  }
-}
-
-// C <- Q^T C (DORMQR 'L','T'): reflectors 0..n-1 of A applied in order.
-// One warp per column of C (n x nc), no block barriers inside.
-__device__ __noinline__ void blk_ormqr_LT(const double *A, int lda, int n, const double *tau, double *C,
-                             int ldc, int nc) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int c = warp; c < nc; c += Z2_WARPS) {
-    double *Cc = C + (size_t)c * ldc;
-    for (int i = 0; i < n; ++i) {
-      const double ti = tau[i];
-      if (ti == 0.0) continue;
-      const double *v = A + (size_t)i * lda;
-      double w = 0.0;
-      for (int r = i + 1 + lane; r < n; r += 32) w += v[r] * Cc[r];
-      w = warp_sum(w) + Cc[i];
-      double tw = ti * w;
-      __syncwarp();
-      if (lane == 0) Cc[i] -= tw;
-      for (int r = i + 1 + lane; r < n; r += 32) Cc[r] -= v[r] * tw;
-      __syncwarp();
-    }
-  }
-  __syncthreads();
-}
-
-// C <- C Q (DORMQR 'R','N'): C is nr x n, one warp per row.
-__device__ __noinline__ void blk_ormqr_RN(const double *A, int lda, int n, const double *tau, double *C,
-                             int ldc, int nr) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int r = warp; r < nr; r += Z2_WARPS) {
-    for (int i = 0; i < n; ++i) {
-      const double ti = tau[i];
-      if (ti == 0.0) continue;
-      const double *v = A + (size_t)i * lda;
-      double w = 0.0;
-      for (int k = i + 1 + lane; k < n; k += 32) w += C[r + (size_t)k * ldc] * v[k];
-      w = warp_sum(w) + C[r + (size_t)i * ldc];
-      double tw = ti * w;
-      __syncwarp();
-      if (lane == 0) C[r + (size_t)i * ldc] -= tw;
-      for (int k = i + 1 + lane; k < n; k += 32) C[r + (size_t)k * ldc] -= tw * v[k];
-      __syncwarp();
-    }
-  }
-  __syncthreads();
-}
-
-// Solve R X = C in place (DTRSM 'L','U','N','N'), one warp per column.
-__device__ __noinline__ void blk_trsm_LUN(const double *R, int ldr, int n, double *C, int ldc, int nc) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int c = warp; c < nc; c += Z2_WARPS) {
-    double *Cc = C + (size_t)c * ldc;
-    for (int k = n - 1; k >= 0; --k) {
-      __syncwarp();
-      double bk = Cc[k];
-      if (bk != 0.0) {
-        bk = bk / R[k + (size_t)k * ldr];
-        __syncwarp();
-        if (lane == 0) Cc[k] = bk;
-        const double *Rk = R + (size_t)k * ldr;
-        for (int i = lane; i < k; i += 32) Cc[i] -= bk * Rk[i];
-      }
-    }
-  }
-  __syncthreads();
-}
-
-// Solve X R^T = C in place (DTRSM 'R','U','T','N'), one warp per row.
-__device__ __noinline__ void blk_trsm_RUT(const double *R, int ldr, int n, double *C, int ldc, int nr) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int r = warp; r < nr; r += Z2_WARPS) {
-    for (int k = n - 1; k >= 0; --k) {
-      __syncwarp();
-      double t = 1.0 / R[k + (size_t)k * ldr];
-      double bk = t * C[r + (size_t)k * ldc];
-      __syncwarp();
-      if (lane == 0) C[r + (size_t)k * ldc] = bk;
-      const double *Rk = R + (size_t)k * ldr;
-      for (int j = lane; j < k; j += 32) {
-        double a = Rk[j];
-        if (a != 0.0) C[r + (size_t)j * ldc] -= a * bk;
-      }
-    }
-  }
-  __syncthreads();
-}
-
 // Row / column permutations with 1-based pivots (ZLAPMR, ZLAPMT).
 // forward row: dst(i,:) = src(jpvt(i),:) ; backward row: dst(jpvt(i),:) = src(i,:)
 __device__ __noinline__ void blk_perm_rows(double *dst, int ldd, const double *src, int lds, int n, int nc,
@@ -363,77 +248,11 @@ __device__ __noinline__ void blk_perm_cols(double *dst, int ldd, const double *s
   __syncthreads();
 }
 
-// ---------------------------------------------------------------------------
-// Tiled GEMM: C = alpha op(A) op(B) + beta C, op(X) = X or X^T.
-// triA / triB: treat the stored A / B as upper triangular (entries below the
-// diagonal of the stored matrix read as zero) -- used for TRMM with the R
-// factor whose lower part holds reflectors.
-// Staging buffer: 2 * (Z2_GEMM_TK * (Z2_GEMM_TM + 1)) doubles.
-// ---------------------------------------------------------------------------
-struct GemmOp {
-  const double *A; int lda; bool ta; bool triA;
-  const double *B; int ldb; bool tb; bool triB;
-};
-
 __device__ __forceinline__ double ld_op(const double *X, int ld, bool t, bool tri, int r, int c) {
   // element (r, c) of op(X)
   int sr = t ? c : r, sc = t ? r : c;
   if (tri && sr > sc) return 0.0;
   return X[sr + (size_t)sc * ld];
-}
-
-__device__ __noinline__ void blk_gemm(int m, int n, int k, double alpha, GemmOp op, double beta, double *C,
-                         int ldc, double *tile) {
-  double *As = tile;                                   // [TK][TM+1]
-  double *Bs = tile + Z2_GEMM_TK * (Z2_GEMM_TM + 1);   // [TK][TN+1]
-  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;   // 16 x 16 threads, 4x4 each
-  for (int i0 = 0; i0 < m; i0 += Z2_GEMM_TM)
-    for (int j0 = 0; j0 < n; j0 += Z2_GEMM_TN) {
-      double acc[4][4];
-#pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-      for (int k0 = 0; k0 < k; k0 += Z2_GEMM_TK) {
-        for (int e = threadIdx.x; e < Z2_GEMM_TK * Z2_GEMM_TM; e += Z2_NT) {
-          int r = e % Z2_GEMM_TM, kk = e / Z2_GEMM_TM;
-          int gi = i0 + r, gk = k0 + kk;
-          As[kk * (Z2_GEMM_TM + 1) + r] =
-              (gi < m && gk < k) ? ld_op(op.A, op.lda, op.ta, op.triA, gi, gk) : 0.0;
-        }
-        for (int e = threadIdx.x; e < Z2_GEMM_TK * Z2_GEMM_TN; e += Z2_NT) {
-          int kk = e % Z2_GEMM_TK, c = e / Z2_GEMM_TK;
-          int gk = k0 + kk, gj = j0 + c;
-          Bs[kk * (Z2_GEMM_TN + 1) + c] =
-              (gk < k && gj < n) ? ld_op(op.B, op.ldb, op.tb, op.triB, gk, gj) : 0.0;
-        }
-        __syncthreads();
-#pragma unroll 4
-        for (int kk = 0; kk < Z2_GEMM_TK; ++kk) {
-          double a[4], b[4];
-#pragma unroll
-          for (int q = 0; q < 4; ++q) a[q] = As[kk * (Z2_GEMM_TM + 1) + ty + 16 * q];
-#pragma unroll
-          for (int q = 0; q < 4; ++q) b[q] = Bs[kk * (Z2_GEMM_TN + 1) + tx + 16 * q];
-#pragma unroll
-          for (int x = 0; x < 4; ++x)
-#pragma unroll
-            for (int y = 0; y < 4; ++y) acc[x][y] = fma(a[x], b[y], acc[x][y]);
-        }
-        __syncthreads();
-      }
-#pragma unroll
-      for (int x = 0; x < 4; ++x)
-#pragma unroll
-        for (int y = 0; y < 4; ++y) {
-          int gi = i0 + ty + 16 * x, gj = j0 + tx + 16 * y;
-          if (gi < m && gj < n) {
-            double *cp = C + gi + (size_t)gj * ldc;
-            *cp = (beta == 0.0) ? alpha * acc[x][y] : alpha * acc[x][y] + beta * (*cp);
-          }
-        }
-    }
-  __syncthreads();
 }
 
 // ---------------------------------------------------------------------------
