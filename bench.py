@@ -84,6 +84,31 @@ def adjoint_cost(device: int) -> dict:
             "logdet_grad_ms": g * 1e3, "sweep_ms": s_ * 1e3, "grad_over_sweep": g / s_}
 
 
+def large_batched(device: int) -> dict:
+    """The large batched production configuration: 64 chains, L=16 (N=256),
+    beta=20 at dtau 0.05 (400 slices), h=0.6, Nwrap 8, delayed rank 32
+    requested, time-displaced G(tau,0) for every tau and the momentum-space
+    correlators read back.  One warm-up bin, one timed bin (CUDA events)."""
+    from z2_gauge_zfy_b200 import Chain, Z2Batch
+    chains = [Chain(RT=1.0, J=0.5, h=0.6, mu=0.0, Nlx=16, Nly=16, Ltrot=400, beta=20.0, Nwrap=8,
+                    absolute=1, seed=777 + i) for i in range(64)]
+    with Z2Batch(chains, device=device, delay_k=32, tau=True) as b:
+        b.pre()
+        b.sweep(1, True)
+        ms = b.sweep_timed(1, True)
+        t0 = time.perf_counter()
+        for i in range(len(chains)):
+            b.obs_tau_k(i)
+        tk = time.perf_counter() - t0
+    su = site_updates(chains)
+    return {"workload": "64 chains, L=16 (N=256), beta=20, dtau 0.05, Ltrot 400, h=0.6, K=0.5, "
+                        "Nwrap 8, delayed rank 32 requested (24 fits shared memory), "
+                        "G(tau,0) for all tau + momentum-space correlators",
+            "value": su / (ms / 1e3), "unit": "site-updates/s", "ms_per_bin": ms,
+            "tau_rate": len(chains) * 256 * 400 / (ms / 1e3), "tau_rate_unit": "(site, tau)/s",
+            "momentum_readback_ms": tk * 1e3}
+
+
 def site_updates(chains) -> int:
     return sum(2 * c.N * c.Ltrot for c in chains)
 
@@ -361,6 +386,7 @@ def main():
                                 "batched_over_single_per_gpu": (value / world) / sv}
     if rank == 0 and not args.no_single:
         line["adjoint"] = adjoint_cost(local)
+        line["large_batched"] = large_batched(local)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample()
     if rank == 0:

@@ -211,7 +211,8 @@ __device__ __noinline__ void dev_stab_green_big(const Smem &s, int N, const doub
   // invVRVL = (VR VL)^-1  -> W0
   {
     blk_dmma(N, N, N, 1.0, MatRef{VR, 1, N}, false, MatRef{VL, 1, N}, false, 0.0, W0, N);
-    blk_inverse(W0, N, N, W1, N, ipiv, s.red, s.flag);
+    blk_inverse_blocked(W0, N, N, W1, N, ipiv, s.red, s.flag, s.tile,
+                        s.tile_doubles);
   }
   // invULUR = UR^T UL^T -> W1
   {
@@ -256,9 +257,11 @@ __device__ __noinline__ void dev_stab_green_big(const Smem &s, int N, const doub
   blk_trsm_lun_blocked(B2, n2, n2, B3, n2, n2);
   // invVUR -> W2, invVUL -> W3
   blk_copy(W2, N, VR, N, N, N);
-  blk_inverse(W2, N, N, W0, N, ipiv, s.red, s.flag);
+  blk_inverse_blocked(W2, N, N, W0, N, ipiv, s.red, s.flag, s.tile,
+                        s.tile_doubles);
   blk_copy(W3, N, VL, N, N, N);
-  blk_inverse(W3, N, N, W0, N, ipiv, s.red, s.flag);
+  blk_inverse_blocked(W3, N, N, W0, N, ipiv, s.red, s.flag, s.tile,
+                        s.tile_doubles);
   // mat_left = diag(invVUR, invUUL) invbigV -> B0
   {
     blk_dmma(N, n2, N, 1.0, MatRef{W2, 1, N}, false, MatRef{B3, 1, n2}, false, 0.0, B0, n2);

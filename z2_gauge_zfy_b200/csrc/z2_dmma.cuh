@@ -489,6 +489,146 @@ __device__ __noinline__ void blk_geqrf(double *A, int lda, int n, double *tau, d
   }
 }
 
+// Solve L Z = Y in place, L unit lower triangular (below the diagonal of L),
+// Y n x nc: blocks of 8 rows from the top, the 8 x 8 diagonal block solved one
+// thread per column in registers, the rows below updated by DMMA.
+__device__ __noinline__ void blk_trsm_lln_blocked(const double *L, int ldl, int n, double *Y,
+                                                  int ldy, int nc) {
+  for (int k0 = 0; k0 < n; k0 += 8) {
+    const int kb = (n - k0) < 8 ? (n - k0) : 8;
+    double ll[8][8];
+#pragma unroll
+    for (int p = 0; p < 8; ++p)
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        ll[p][q] = (p > q && p < kb) ? L[(k0 + p) + (size_t)(k0 + q) * ldl] : 0.0;
+    for (int j = threadIdx.x; j < nc; j += Z2_NT) {
+      double *Yj = Y + (size_t)j * ldy + k0;
+      double y[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) y[q] = (q < kb) ? Yj[q] : 0.0;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const double z = y[q];
+#pragma unroll
+        for (int p = 0; p < 8; ++p)
+          if (p > q) y[p] -= z * ll[p][q];
+      }
+#pragma unroll
+      for (int q = 0; q < 8; ++q) if (q < kb) Yj[q] = y[q];
+    }
+    __syncthreads();
+    if (k0 + kb < n) {
+      blk_dmma(n - k0 - kb, nc, kb, -1.0, MatRef{L + (k0 + kb) + (size_t)k0 * ldl, 1, ldl}, false,
+               MatRef{Y + k0, 1, ldy}, false, 1.0, Y + k0 + kb, ldy);
+    }
+  }
+}
+
+__device__ __noinline__ void blk_trsm_lun_blocked(const double *R, int ldr, int n, double *Y,
+                                                  int ldy, int nc);
+
+// Inverse of a general n x n matrix by LU with partial pivoting (the
+// ZGEFA/ZGEDI pair of INV_C, lib/package_of_matrix/Modules/mat_mod.f90:296-336),
+// blocked: panels of 16 columns (pivot search over the column, full-row
+// interchanges, in-panel rank-1 updates one warp per column), U12 = L11^-1 A12
+// one thread per column (L11 staged in work), A22 -= L21 U12 by DMMA; then
+// A^-1 = U^-1 L^-1 P from the identity by the two blocked triangular solves.
+// A is overwritten by its inverse; W (ldw) is an n x n workspace; work holds
+// >= 256 doubles of shared memory (else the unblocked blk_inverse runs).
+__device__ __noinline__ void blk_inverse_blocked(double *A, int lda, int n, double *W, int ldw,
+                                                 int *ipiv, double *red, int *flag, double *work,
+                                                 int wd) {
+  if (work == nullptr || wd < 256) {
+    blk_inverse(A, lda, n, W, ldw, ipiv, red, flag);
+    return;
+  }
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int j0 = 0; j0 < n; j0 += 16) {
+    const int jb = (n - j0) < 16 ? (n - j0) : 16;
+    for (int k = j0; k < j0 + jb; ++k) {
+      double bv = -1.0; int bi = n;
+      for (int i = k + tid; i < n; i += Z2_NT) {
+        const double v = fabs(A[i + (size_t)k * lda]);
+        if (v > bv) { bv = v; bi = i; }
+      }
+#pragma unroll
+      for (int o = 16; o; o >>= 1) {
+        const double ov = __shfl_xor_sync(Z2_FULL, bv, o);
+        const int oi = __shfl_xor_sync(Z2_FULL, bi, o);
+        if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+      }
+      if (lane == 0) { red[warp] = bv; flag[warp] = bi; }
+      __syncthreads();
+      bv = red[0]; bi = flag[0];
+      for (int w = 1; w < Z2_WARPS; ++w)
+        if (red[w] > bv || (red[w] == bv && flag[w] < bi)) { bv = red[w]; bi = flag[w]; }
+      const int p = bi;
+      __syncthreads();
+      if (tid == 0) ipiv[k] = p;
+      if (p != k)
+        for (int j = tid; j < n; j += Z2_NT) {
+          const double t = A[k + (size_t)j * lda];
+          A[k + (size_t)j * lda] = A[p + (size_t)j * lda];
+          A[p + (size_t)j * lda] = t;
+        }
+      __syncthreads();
+      const double piv = A[k + (size_t)k * lda];
+      for (int i = k + 1 + tid; i < n; i += Z2_NT) A[i + (size_t)k * lda] /= piv;
+      __syncthreads();
+      for (int j = k + 1 + warp; j < j0 + jb; j += Z2_WARPS) {
+        const double akj = A[k + (size_t)j * lda];
+        if (akj != 0.0)
+          for (int i = k + 1 + lane; i < n; i += 32) A[i + (size_t)j * lda] -= A[i + (size_t)k * lda] * akj;
+      }
+      __syncthreads();
+    }
+    const int nc = n - j0 - jb;
+    if (nc <= 0) continue;
+    // U12 = L11^-1 A12 (L11 unit lower, staged in shared memory)
+    for (int e = tid; e < jb * jb; e += Z2_NT) {
+      const int p = e % jb, q = e / jb;
+      work[p + 16 * q] = (p > q) ? A[(j0 + p) + (size_t)(j0 + q) * lda] : 0.0;
+    }
+    __syncthreads();
+    for (int c = tid; c < nc; c += Z2_NT) {
+      double *Ac = A + j0 + (size_t)(j0 + jb + c) * lda;
+      double y[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) y[q] = (q < jb) ? Ac[q] : 0.0;
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const double z = y[q];
+#pragma unroll
+        for (int p = 0; p < 16; ++p)
+          if (p > q) y[p] -= z * work[p + 16 * q];
+      }
+#pragma unroll
+      for (int q = 0; q < 16; ++q) if (q < jb) Ac[q] = y[q];
+    }
+    __syncthreads();
+    // A22 -= L21 U12
+    blk_dmma(n - j0 - jb, nc, jb, -1.0, MatRef{A + (j0 + jb) + (size_t)j0 * lda, 1, lda}, false,
+             MatRef{A + j0 + (size_t)(j0 + jb) * lda, 1, lda}, false, 1.0,
+             A + (j0 + jb) + (size_t)(j0 + jb) * lda, lda);
+  }
+  // W = P I (row interchanges of the factorization, in order)
+  blk_identity(W, ldw, n);
+  for (int c = tid; c < n; c += Z2_NT)
+    for (int k = 0; k < n; ++k) {
+      const int p = ipiv[k];
+      if (p != k) {
+        const double t = W[k + (size_t)c * ldw];
+        W[k + (size_t)c * ldw] = W[p + (size_t)c * ldw];
+        W[p + (size_t)c * ldw] = t;
+      }
+    }
+  __syncthreads();
+  blk_trsm_lln_blocked(A, lda, n, W, ldw, n);   // L^-1 P
+  blk_trsm_lun_blocked(A, lda, n, W, ldw, n);   // U^-1 L^-1 P
+  blk_copy(A, lda, W, ldw, n, n);
+}
+
 // Solve R Z = Y in place (DTRSM 'L','U','N','N'), Y n x nc (ldy), R upper
 // (ldr).  Blocks of 8 rows from the bottom: the 8 x 8 diagonal block is
 // solved one thread per column (block of R held in registers), the rows
