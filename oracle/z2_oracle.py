@@ -42,6 +42,7 @@ from dataclasses import dataclass, field
 import numpy as np
 from scipy.linalg import blas, lapack
 
+RATIO_EPS = 1.0e-300   # src/globalK.f90:9
 ZERO = 1.0e-10          # src/calc_basic.f90:5
 UPBOUND = 1.0e200       # src/calc_basic.f90:7
 IP_RANF = 48828125      # lib/package_of_matrix/Ran/ran_imada.f:60
@@ -569,6 +570,13 @@ class WrapList:
         self.DLlist = np.zeros((Nst + 1, N))
 
 
+def _wrlist_copy(wr: "WrapList") -> "WrapList":
+    c = WrapList.__new__(WrapList)
+    for k, v in wr.__dict__.items():
+        c.__dict__[k] = v.copy()
+    return c
+
+
 class PropGreen:
     """``PropGreen`` (src/process_matrix.f90:17-24, 68-96)."""
 
@@ -990,6 +998,12 @@ class Z2Chain:
         self.decisions = []
         self.ratios = []
         self.dyn_X = (np.zeros(3), np.zeros(3))
+        # global update state (src/global_update.f90, src/main.f90:74-76)
+        self.is_beta = True
+        self.gacc = 0.0          # Acc_Kg%acc
+        self.gsize = 0.0         # Wolff%size_cluster
+        self.g_last = (0, 0)     # (accepted, proposed) of the last Global_sweep
+        self.g_log = []          # (bond, size, log ratio space, fermion, accept) per move
 
     # ---- LocalK (src/localK.f90) ------------------------------------------
     def metro(self, ii: int, nt: int):
@@ -1171,13 +1185,173 @@ class Z2Chain:
         self.nobs = 0
         self.nobst = 0
         for _ in range(self.p.Nsweep if nsweep is None else nsweep):
-            self.sweep_L()
-            self.sweep_R(toggle)
+            if self.is_beta:
+                self.sweep_L()
+                self.sweep_R(toggle)
+            else:
+                self.sweep_R(toggle)
+                self.sweep_L()
         self.obs.ave(self.nobs)
         if toggle:
             self.obs_tau.ave(self.nobst)
         if self.acc_den > 0.0:
             self.acc += self.acc_num / self.acc_den
+
+    # ---- Global Wolff-in-tau move (src/global_update.f90, src/globalK.f90) --
+    def nranf(self, N: int) -> int:
+        """``nranf`` (src/calc_basic.f90:113-121): nint(ranf*N + 0.5),
+        clamped to 1..N (1-based)."""
+        x = self.rng() * float(N) + 0.5
+        n = math.floor(x)
+        if x - n >= 0.5:          # nint rounds half away from zero (x >= 0)
+            n += 1
+        return int(min(max(n, 1), N))
+
+    def time_bond_prob(self) -> float:
+        """``compute_time_bond_prob`` (src/global_update.f90:88-101)."""
+        p = self.p
+        if abs(p.h) > ZERO:
+            ta = max(math.tanh(p.dtau * abs(p.h)), RATIO_EPS)
+            gamma = -0.5 * math.log(ta)
+            pt = 1.0 - math.exp(-2.0 * gamma)
+        else:
+            pt = 0.0
+        return max(0.0, min(1.0, pt))
+
+    def wolff_flip(self, sigma_new):
+        """``Wolff_flip`` (src/global_update.f90:66-86): a time cluster on
+        one bond, its plaquette log ratio, the flip applied to sigma_new.
+        Returns (bond 0-based, cluster size, log ratio space)."""
+        p = self.p
+        L = p.Ltrot
+        b = self.nranf(2 * p.Lq) - 1
+        pt = self.time_bond_prob()
+        # build_time_cluster (src/global_update.f90:103-131), 0-based tau
+        mask = np.zeros(L, dtype=bool)
+        q0 = self.nranf(L) - 1
+        queue = [q0]
+        mask[q0] = True
+        head = 0
+        while head < len(queue):
+            cur = queue[head]
+            head += 1
+            for off in (-1, 1):
+                nb = (cur + off) % L
+                if mask[nb]:
+                    continue
+                if sigma_new[b, nb] == sigma_new[b, cur]:
+                    # the reference evaluates ranf only when p_time > 0
+                    if pt > 0.0 and self.rng() < pt:
+                        queue.append(nb)
+                        mask[nb] = True
+        size = int(mask.sum())
+        if size == 0:
+            return b, 0, 0.0
+        # compute_space_log_ratio / plaquette_log_ratio (src/global_update.f90:133-172)
+        lrs = 0.0
+        alpha = p.dtau * p.J
+        if alpha != 0.0:
+            bb = self.lat.bond_bonds
+            for tau in range(L):
+                if not mask[tau]:
+                    continue
+                for start in (1, 4):
+                    prod = sigma_new[b, tau]
+                    for k in range(3):
+                        prod = prod * sigma_new[bb[b, start + k], tau]
+                    lrs += -2.0 * alpha * prod
+        sigma_new[b, mask] = -sigma_new[b, mask]   # apply_cluster_flip
+        self._gmask = mask
+        return b, size, lrs
+
+    def ratio_k_fermion(self, sigma_new, ii: int, nt: int) -> float:
+        """``ratioK_fermion`` (src/globalK.f90:15-113): |det Prod|^2 for the
+        change sigma -> sigma_new at (ii, nt) and the G update; nt 0-based."""
+        s_old = self.sigma[ii, nt]
+        s_new = sigma_new[ii, nt]
+        if s_new == s_old:
+            return 1.0
+        G = self.prop.Gr
+        p1, p2 = self.lat.bond_list[ii]
+        P = (p1, p2)
+        Dl = self.opk.get_delta(ii, s_old, s_new)
+        Gl = np.empty((2, 2), dtype=G.dtype)
+        for nr in range(2):
+            for nl in range(2):
+                Gl[nl, nr] = (1.0 if nl == nr else 0.0) - G[P[nl], P[nr]]
+        prod = np.empty((2, 2), dtype=G.dtype)
+        for nr in range(2):
+            for nl in range(2):
+                m = Dl[nl, 0] * Gl[0, nr] + Dl[nl, 1] * Gl[1, nr]
+                prod[nl, nr] = (1.0 if nl == nr else 0.0) + m
+        det = prod[0, 0] * prod[1, 1] - prod[0, 1] * prod[1, 0]
+        ratio = max(abs(det * det), RATIO_EPS)
+        pinv = np.array([[prod[1, 1], -prod[0, 1]], [-prod[1, 0], prod[0, 0]]]) / det
+        U = G[:, [p1, p2]].copy()
+        V = np.empty((2, G.shape[0]), dtype=G.dtype)
+        for no in range(2):
+            V[no, :] = -Dl[no, 0] * G[p1, :] - Dl[no, 1] * G[p2, :]
+            V[no, p1] += Dl[no, 0]
+            V[no, p2] += Dl[no, 1]
+        self.prop.Gr = G - (U @ pinv) @ V
+        return float(ratio)
+
+    def _global_move(self, left: bool):
+        """``Global_sweep_L`` / ``Global_sweep_R`` (src/global_update.f90:228-318)
+        on copies of the propagator and wrap lists."""
+        p = self.p
+        sigma_new = self.sigma.copy()
+        b, size, lrs = self.wolff_flip(sigma_new)
+        keep_prop, keep_wr = self.prop, self.wr
+        self.prop, self.wr = keep_prop.copy(), _wrlist_copy(keep_wr)
+        lrf = 0.0
+        pr = self.prop
+        if left:
+            for nt in range(p.Ltrot, 0, -1):
+                if nt % p.Nwrap == 0:
+                    self.wrap_L(nt, flag=False)
+                self.propT_L()
+                for ii in range(2 * p.Lq - 1, -1, -1):   # GlobalK_prop_L (globalK.f90:115-133)
+                    lrf += math.log(max(self.ratio_k_fermion(sigma_new, ii, nt - 1), RATIO_EPS))
+                self.opk.mmult_L(pr.Gr, sigma_new, nt - 1, 1)
+                self.opk.mmult_R(pr.Gr, sigma_new, nt - 1, -1)
+                self.opk.mmult_L(pr.UUL, sigma_new, nt - 1, 1)
+            self.wrap_L(0, flag=False)
+        else:
+            self.wrap_R(0, flag=False)
+            for nt in range(1, p.Ltrot + 1):
+                self.opk.mmult_R(pr.Gr, self.sigma, nt - 1, 1)   # GlobalK_prop_R (globalK.f90:135-153)
+                self.opk.mmult_L(pr.Gr, self.sigma, nt - 1, -1)
+                for ii in range(2 * p.Lq):
+                    lrf += math.log(max(self.ratio_k_fermion(sigma_new, ii, nt - 1), RATIO_EPS))
+                self.opk.mmult_R(pr.UUR, sigma_new, nt - 1, 1)
+                self.propT_R()
+                if nt % p.Nwrap == 0:
+                    self.wrap_R(nt, flag=False)
+        lrt = lrf + lrs
+        r = self.rng()
+        accept = min(0.0, lrt) >= math.log(max(r, RATIO_EPS))
+        if accept:
+            self.sigma = sigma_new
+            self.is_beta = not left
+        else:
+            self.prop, self.wr = keep_prop, keep_wr
+        self.g_log.append((b, size, lrs, lrf, bool(accept)))
+        return accept, size
+
+    def global_sweep(self, nglobal: int):
+        """``Global_sweep`` (src/global_update.f90:320-337): Nglobal Wolff
+        moves, each followed by a trial half-sweep in the current direction."""
+        num = 0
+        size = 0.0
+        for _ in range(nglobal):
+            acc, sz = self._global_move(self.is_beta)
+            num += int(acc)
+            size += float(sz)
+        self.g_last = (num, nglobal)
+        if nglobal > 0:
+            self.gacc += num / nglobal
+            self.gsize += size / nglobal
 
     # ---- Dynamics (src/dynamics.f90) ---------------------------------------
     def dyn_sweep(self):

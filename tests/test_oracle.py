@@ -166,3 +166,47 @@ def test_read_params_format(tmp_path):
     assert (p.RT, p.J, p.h, p.mu, p.Q) == (0.5, 1.0, 0.52, 0.3, 1.0)
     assert (p.Nlx, p.Nly, p.Ltrot, p.beta, p.Nwrap) == (4, 4, 80, 20.0, 4)
     assert p.dtau == 0.25 and p.Nst == 20 and p.absolute == 5 and not p.is_tau
+
+
+def _dense_G(c):
+    p = c.p
+    B = np.eye(p.Lq)
+    for nt in range(p.Ltrot):
+        B = (c.opk.dense_B(c.sigma, nt) * c.opmu.expMU_P) @ B
+    return np.linalg.inv(np.eye(p.Lq) + B)
+
+
+def test_nranf_rounding():
+    class Fixed:
+        def __init__(self, v):
+            self.v = v
+
+        def __call__(self):
+            return self.v
+    c = zo.Z2Chain(zo.Params(RT=1.0, J=0.5, h=0.5, Nlx=2, Nly=2, Ltrot=4, beta=0.4, Nwrap=2))
+    for v, N, want in ((0.0, 8, 1), (0.999999, 8, 8), (0.25, 8, 3), (0.3125, 8, 3),
+                       (0.375, 8, 4), (0.5, 3, 2)):
+        c.rng = Fixed(v)
+        assert c.nranf(N) == want, (v, N)
+
+
+def test_global_moves_keep_G_consistent():
+    """Global Wolff-in-tau moves (src/global_update.f90): after each move the
+    current G is (I + B_Ltrot ... B_1)^-1 of the current sigma (up to the
+    drift of the flips), moves are both accepted and rejected, and the
+    direction flag flips on every accepted move."""
+    p = zo.Params(RT=1.0, J=0.5, h=0.3, mu=0.1, Nlx=4, Nly=4, Ltrot=20, beta=2.0, Nwrap=5)
+    c = zo.Z2Chain(p, seed=4242)
+    c.pre()
+    seen = set()
+    for _ in range(6):
+        beta_before = c.is_beta
+        c.global_sweep(1)
+        acc = c.g_log[-1][4]
+        seen.add(acc)
+        assert c.is_beta == (beta_before if not acc else not beta_before)
+        G = _dense_G(c)
+        assert np.max(np.abs(c.prop.Gr - G)) < 1e-6
+        c.sweep()
+    assert seen == {True, False}
+    assert 0.0 <= c.gacc <= 6.0
