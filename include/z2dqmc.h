@@ -132,6 +132,21 @@ int z2_set_replay(z2_handle *h, int32_t chain, const double *r, size_t n);
  * accepted-flip X/Y columns, pending slice products, UDV stack copies. */
 #define Z2_NPHASE 12
 int z2_get_phase_cycles(const z2_handle *h, int32_t chain, double out[Z2_NPHASE]);
+/* Global Wolff-in-tau moves: Global_sweep (src/global_update.f90:320-337)
+ * for every chain, nglobal moves each.  A move picks a bond and grows a
+ * cluster of its links along tau (build_time_cluster, :103-131, flip
+ * probability 1 - tanh(dtau h)), adds the plaquette log ratio (:133-172),
+ * runs a trial half-sweep in the chain's current direction with the
+ * cluster's links flipped (GlobalK_prop_L/R, src/globalK.f90:115-153) and
+ * accepts with min(1, ratio); an accepted move reverses the direction of the
+ * next bin (is_beta, src/main.f90:73-77; z2_sweep honours it).  The first
+ * call allocates a backup of each chain's state that a rejected move
+ * restores.  Call after z2_pre. */
+int z2_sweep_global(z2_handle *h, int32_t nglobal);
+/* out[5]: Acc_Kg%acc (sum over calls of the accepted fraction), Wolff
+ * size_cluster (sum over calls of the mean cluster size), accepted and
+ * proposed moves of the last call, is_beta (1 or 0). */
+int z2_get_global_stats(const z2_handle *h, int32_t chain, double out[5]);
 /* Delay-rank autotuner (no reference counterpart: the reference applies each
  * accepted flip to G at once, src/localK.f90:141-165).  For every distinct
  * lattice size among params[0..nchains) it times one bin of short probe

@@ -111,3 +111,32 @@ def test_driver_tau_momentum_files(tmp_path):
         assert np.allclose(got, ref, rtol=1e-9, atol=1e-12), f
     for f in ("sdw_susc", "curxx_freq", "curxx_L_tau", "g_r0_tau", "pair_s_zero_tau"):
         assert (tmp_path / f).stat().st_size > 0, f
+
+
+def test_driver_global_moves(tmp_path):
+    """is_global: Nglobal Wolff moves before every bin (src/main.f90:76),
+    per-bin observables against the oracle doing the same."""
+    build.build()
+    params = PARAMS.replace(".false. 0\n.false. 0\n.false. 0\n", ".false. 0\n.false. 0\n.true. 2\n")
+    (tmp_path / "paramC_sets.txt").write_text(params)
+    (tmp_path / "confin.txt").write_text("0\n")
+    (tmp_path / "seeds.txt").write_text("12345\n")
+    r = subprocess.run([build.DRIVER, "--chains", "1", "--dir", str(tmp_path)],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    p = zo.read_params(str(tmp_path / "paramC_sets.txt"))
+    assert p.is_global and p.Nglobal == 2
+    c = zo.Z2Chain(p, seed=12345)
+    c.pre()
+    ref = {k: [] for k in ("flux_avg", "chi_flux", "pair_sc_q0", "cdw_pi", "cdw_ratio", "density")}
+    for _ in range(p.Nbin):
+        c.global_sweep(p.Nglobal)
+        c.sweep()
+        d = c.obs.as_dict()
+        for k in ref:
+            ref[k].append(d[k])
+    for k, v in ref.items():
+        got = np.array([float(x) for x in (tmp_path / k).read_text().split()])
+        assert np.allclose(got, np.array(v), rtol=1e-10, atol=1e-12), k
+    info = (tmp_path / "info.txt").read_text()
+    assert "Accept_Kglobal" in info and "Wolff cluster" in info

@@ -231,6 +231,16 @@ class Z2Batch:
         a = (re + 1j * im).reshape(7, L, N)
         return {k: a[q].T.copy() for q, k in enumerate(OBS_TAU_NAMES)}
 
+    def sweep_global(self, nglobal: int):
+        """Global Wolff-in-tau moves of every chain (``z2_sweep_global``,
+        Sweep_global%sweep of the reference)."""
+        self._c(self.lib.z2_sweep_global(self.h, nglobal))
+
+    def global_stats(self, chain: int) -> dict:
+        buf = np.empty(5)
+        self._c(self.lib.z2_get_global_stats(self.h, chain, dptr(buf)))
+        return dict(zip(("acc", "size_cluster", "accepted", "proposed", "is_beta"), buf.tolist()))
+
     def stats(self, chain: int) -> dict:
         buf = np.empty(_ffi.Z2_NSTATS)
         self._c(self.lib.z2_get_stats(self.h, chain, dptr(buf)))

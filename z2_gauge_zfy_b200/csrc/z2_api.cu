@@ -15,7 +15,7 @@
 
 static_assert(PH_COUNT == Z2_NPHASE, "phase counters and the C ABI disagree");
 
-enum { OP_PRE = 1, OP_SWEEP = 2, OP_LOGDET = 3 };
+enum { OP_PRE = 1, OP_SWEEP = 2, OP_LOGDET = 3, OP_GLOBAL = 4 };
 enum { U_MMULT_R = 1, U_MMULT_L, U_STAB_UR, U_STAB_UL, U_STAB_GREEN, U_STAB_GREEN_BIG };
 
 struct UnitArgs {
@@ -61,6 +61,8 @@ z2_chain_kernel(const ChainDesc *descs, const int *order, int nchains, int *queu
       chain_sweep(sc, s, nsweep, toggle != 0, sc.hzero ? 1.0 : 0.0);
     } else if (op == OP_LOGDET) {
       chain_logdet_grad(sc, s);
+    } else if (op == OP_GLOBAL) {
+      chain_global(sc, s, nsweep);
     }
     __syncthreads();
   }
@@ -199,6 +201,7 @@ struct ChainHost {
   double *replay = nullptr;
   double *ktab = nullptr;            // [2][N][N] cos, sin of k.r (tau chains only)
   double *kout = nullptr;            // [2][7][Ltrot][N] k-space correlators
+  char *gbase = nullptr;             // global-move backup block
 };
 
 }  // namespace
@@ -516,6 +519,17 @@ extern "C" int z2_create(z2_handle **out, const z2_chain_params *params, int32_t
     d.rt_scalar = p.RT;
     for (int q = 0; q < 9; ++q) d.rb[q] = rb[q];
     d.use_kin = p.RT > kZero ? 1 : 0;
+    // global moves: dtau J of the plaquette ratio and the time-bond
+    // probability of compute_time_bond_prob (src/global_update.f90:88-101)
+    d.alphaJ = C.dtau * p.J;
+    {
+      double pt = 0.0;
+      if (std::fabs(p.h) > kZero) {
+        const double ta = std::max(std::tanh(C.dtau * std::fabs(p.h)), 1.0e-300);
+        pt = 1.0 - std::exp(-2.0 * (-0.5 * std::log(ta)));
+      }
+      d.ptime = std::max(0.0, std::min(1.0, pt));
+    }
     d.hzero = std::fabs(p.h) <= kZero ? 1 : 0;
     d.bonds = (const int *)(base + o_bonds); d.groups = (const int *)(base + o_groups);
     d.bbonds = (const int *)(base + o_bb); d.plaq = (const int *)(base + o_plaq);
@@ -587,6 +601,7 @@ extern "C" int z2_destroy(z2_handle *h) {
   for (auto &C : h->ch) {
     if (C.base) cudaFree(C.base);
     if (C.replay) cudaFree(C.replay);
+    if (C.gbase) cudaFree(C.gbase);
   }
   if (h->d_desc) cudaFree(h->d_desc);
   if (h->d_order) cudaFree(h->d_order);
@@ -785,6 +800,48 @@ extern "C" int z2_get_obs_tau_k(const z2_handle *h, int32_t chain, double *re, d
   CUDA_TRY(hh, cudaMemcpyAsync(re, C.kout, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(hh, cudaMemcpyAsync(im, C.kout + n, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(hh, cudaStreamSynchronize(h->stream));
+  return Z2_OK;
+}
+
+static int upload_desc(z2_handle *h, int chain);
+
+// Global_sweep for every chain (src/global_update.f90:320-337).  The backup
+// of the chain state that a rejected move restores is allocated on the first
+// call.
+extern "C" int z2_sweep_global(z2_handle *h, int32_t nglobal) {
+  if (!h) return Z2_ERR_ARG;
+  if (nglobal < 0) return set_err(h, Z2_ERR_ARG, "z2_sweep_global: nglobal = %d", nglobal);
+  if (!h->pre_done) return set_err(h, Z2_ERR_STATE, "z2_sweep_global before z2_pre");
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  for (int c = 0; c < h->nchains; ++c) {
+    ChainHost &C = h->ch[c];
+    if (C.gbase) continue;
+    const size_t NN = (size_t)C.N * C.N, S1 = (size_t)C.Nst + 1;
+    const size_t nd = 5 * NN + 2 * (size_t)C.N + 4 * NN * S1 + 2 * (size_t)C.N * S1 + 1;
+    const size_t bytes = al256(8 * nd) + al256((size_t)C.Ltrot) + al256(4 * (size_t)C.Ltrot);
+    char *b = nullptr;
+    if (cudaMalloc(&b, bytes) != cudaSuccess)
+      return set_err(h, Z2_ERR_NOMEM, "chain %d: cudaMalloc of %zu bytes failed", c, bytes);
+    C.gbase = b;
+    C.d.gbak = (double *)b;
+    C.d.gmask = (signed char *)(b + al256(8 * nd));
+    C.d.gqueue = (int *)(b + al256(8 * nd) + al256((size_t)C.Ltrot));
+    int r = upload_desc(h, c);
+    if (r) return r;
+  }
+  if (nglobal == 0) return Z2_OK;
+  return launch_chains(h, OP_GLOBAL, nglobal, 0, nullptr);
+}
+
+extern "C" int z2_get_global_stats(const z2_handle *h, int32_t chain, double out[5]) {
+  int r = check_chain(h, chain);
+  if (r) return r;
+  z2_handle *hh = const_cast<z2_handle *>(h);
+  double a[A_COUNT];
+  CUDA_TRY(hh, cudaSetDevice(h->device));
+  CUDA_TRY(hh, cudaMemcpy(a, h->ch[chain].d.acc, sizeof(a), cudaMemcpyDeviceToHost));
+  out[0] = a[A_GACC]; out[1] = a[A_GSIZE]; out[2] = a[A_GNUM]; out[3] = a[A_GDEN];
+  out[4] = a[A_NOTBETA] == 0.0 ? 1.0 : 0.0;
   return Z2_OK;
 }
 

@@ -21,6 +21,10 @@ enum {
   A_TXMAX0, A_TXMAX1, A_TXMAX2, A_TXMEAN0, A_TXMEAN1, A_TXMEAN2,
   A_BIN0,                        // 7 bin results: flux_avg .. density
   A_LOGDET = A_BIN0 + 7, A_DMU, A_DRAWS,
+  // global moves (src/global_update.f90): accepted / proposed of the last
+  // Global_sweep, Acc_Kg%acc, Wolff%size_cluster, sweep direction (0: the
+  // next bin runs L then R, the reference's is_beta = .true.)
+  A_GNUM, A_GDEN, A_GACC, A_GSIZE, A_NOTBETA,
   A_PH0,                         // Z2_NPHASE per-phase SM cycle counters
   A_COUNT = A_PH0 + 12
 };
@@ -73,6 +77,13 @@ struct ChainDesc {
   double *B0, *B1, *B2, *B3;                      // 2N x 2N workspaces
   double *obs_tau;      // [7][Ltrot][N]
   double *grad;         // [2N] adjoint output
+  // global moves: state backup (G..VL, DR DL, stacks, Xmaxm), cluster mask
+  // and queue, allocated by the first z2_sweep_global
+  double *gbak;
+  signed char *gmask;   // [Ltrot]
+  int *gqueue;          // [Ltrot]
+  double alphaJ;        // dtau J (plaquette log ratio)
+  double ptime;         // compute_time_bond_prob
   // accumulators
   double *acc;          // [A_COUNT]
   unsigned int *rng;    // ranf state (iseed), always in [0, 2^31)

@@ -75,6 +75,7 @@ __device__ __noinline__ void dyn_sweep(const ChainDesc &c, const Smem &s) {
 // Local_sweep_pre (src/local_sweep.f90:87-104)
 __device__ __noinline__ void chain_pre(const ChainDesc &c, const Smem &s) {
   const int N = c.N;
+  if (threadIdx.x == 0) c.acc[A_NOTBETA] = 0.0;   // is_beta = .true. (src/main.f90:73)
   blk_identity(c.UR, N, N); blk_identity(c.VR, N, N); blk_fill(c.DR, N, 1.0);
   blk_identity(c.ULT, N, N); blk_identity(c.VL, N, N); blk_fill(c.DL, N, 1.0);
   blk_identity(c.G, N, N);
@@ -161,8 +162,13 @@ __device__ __noinline__ void chain_sweep(const ChainDesc &c, const Smem &s, int 
   __syncthreads();
   load_G(c, s);
   for (int n = 0; n < nsweep; ++n) {
-    sweep_L(c, s);
-    sweep_R(c, s, toggle);
+    if (c.acc[A_NOTBETA] == 0.0) {   // is_beta: L then R
+      sweep_L(c, s);
+      sweep_R(c, s, toggle);
+    } else {
+      sweep_R(c, s, toggle);
+      sweep_L(c, s);
+    }
   }
   if (threadIdx.x == 0) {
     // Obs_equal_ave (src/obser_equal.f90:50-71)
@@ -188,6 +194,218 @@ __device__ __noinline__ void chain_sweep(const ChainDesc &c, const Smem &s, int 
     const double z = 1.0 / c.acc[A_NOBST];
     const size_t n = (size_t)7 * c.Ltrot * N;
     for (size_t i = threadIdx.x; i < n; i += Z2_NT) c.obs_tau[i] = z * c.obs_tau[i];
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// Global Wolff-in-tau move (src/global_update.f90, src/globalK.f90)
+// ---------------------------------------------------------------------------
+// nranf (src/calc_basic.f90:113-121): nint(ranf*N + 0.5) clamped to 1..N.
+__device__ __forceinline__ int dev_nranf(unsigned int &st, int N) {
+  st = ranf_adv(st, 1);
+  const double x = (double)st * (1.0 / 2147483648.0) * (double)N + 0.5;
+  long long n = llround(x);            // nint: half away from zero
+  if (n < 1) n = 1;
+  if (n > N) n = N;
+  return (int)n;
+}
+
+// State of the chain that a rejected move restores (Prop_assign and
+// Wrlist_assign, src/process_matrix.f90:58-66, 104-112): G, UR, VR, ULT, VL
+// (contiguous), DR, DL, the four UDV stacks, their D stacks and Xmaxm.
+__device__ __noinline__ void global_backup(const ChainDesc &c, bool save) {
+  const size_t NN = (size_t)c.N * c.N, S1 = (size_t)c.Nst + 1;
+  const size_t n0 = 5 * NN, n1 = 2 * (size_t)c.N, n2 = 4 * NN * S1, n3 = 2 * (size_t)c.N * S1;
+  double *src[4] = {c.G, c.DR, c.URs, c.DRs};
+  double *bak[4] = {c.gbak, c.gbak + n0, c.gbak + n0 + n1, c.gbak + n0 + n1 + n2};
+  const size_t len[4] = {n0, n1, n2, n3};
+  for (int q = 0; q < 4; ++q) {
+    const double *from = save ? src[q] : bak[q];
+    double *to = save ? bak[q] : src[q];
+    for (size_t i = threadIdx.x; i < len[q]; i += Z2_NT) to[i] = from[i];
+  }
+  if (threadIdx.x == 0) {
+    double *x = c.gbak + n0 + n1 + n2 + n3;
+    if (save) *x = c.acc[A_XMAX]; else c.acc[A_XMAX] = *x;
+  }
+  __syncthreads();
+}
+
+// One cluster site of a trial half-sweep (ratioK_fermion, src/globalK.f90:15-113):
+// the bond flips at slice nt if the cluster holds nt; |det Prod|^2 goes into
+// the fermion log ratio (thread 0) and G takes the rank-2 update.
+__device__ __noinline__ void global_flip_slice(const ChainDesc &c, const Smem &s, int nt, int b,
+                                               double &lrf) {
+  if (!c.gmask[nt - 1]) return;
+  const int N = c.N, ldg = s.ldg, ldx = s.ldx;
+  double *G = s.G, *X = s.X, *Yt = s.Yt;
+  signed char *sg = c.sigma + (size_t)(nt - 1) * c.nb;
+  const int p1 = s.bond[2 * b], p2 = s.bond[2 * b + 1];
+  const double s_old = (double)sg[b], s_new = -s_old;
+  const double D11 = c.dlt[2 * b], D12 = s_new * c.dlt[2 * b + 1];
+  const double g11 = G[p1 + (size_t)p1 * ldg], g12 = G[p1 + (size_t)p2 * ldg];
+  const double g21 = G[p2 + (size_t)p1 * ldg], g22 = G[p2 + (size_t)p2 * ldg];
+  const double l11 = __dsub_rn(1.0, g11), l12 = -g12, l21 = -g21, l22 = __dsub_rn(1.0, g22);
+  const double m11 = __dadd_rn(__dmul_rn(D11, l11), __dmul_rn(D12, l21));
+  const double m12 = __dadd_rn(__dmul_rn(D11, l12), __dmul_rn(D12, l22));
+  const double m21 = __dadd_rn(__dmul_rn(D12, l11), __dmul_rn(D11, l21));
+  const double m22 = __dadd_rn(__dmul_rn(D12, l12), __dmul_rn(D11, l22));
+  const double p11 = __dadd_rn(1.0, m11), p12 = m12, p21 = m21, p22 = __dadd_rn(1.0, m22);
+  const double det = __dsub_rn(__dmul_rn(p11, p22), __dmul_rn(p12, p21));
+  if (threadIdx.x == 0) lrf += log(fmax(fabs(__dmul_rn(det, det)), 1.0e-300));
+  const double q00 = p22 / det, q01 = -p12 / det, q10 = -p21 / det, q11 = p11 / det;
+  __syncthreads();   // every thread has read G(P, P)
+  for (int i = threadIdx.x; i < N; i += Z2_NT) {
+    const double u0 = G[i + (size_t)p1 * ldg], u1 = G[i + (size_t)p2 * ldg];
+    const double v0 = G[p1 + (size_t)i * ldg], v1 = G[p2 + (size_t)i * ldg];
+    X[i] = u0 * q00 + u1 * q10;
+    X[i + ldx] = u0 * q01 + u1 * q11;
+    double y0 = -D11 * v0 - D12 * v1;
+    double y1 = -D12 * v0 - D11 * v1;
+    if (i == p1) { y0 += D11; y1 += D12; }
+    if (i == p2) { y0 += D12; y1 += D11; }
+    Yt[i] = y0;
+    Yt[i + ldx] = y1;
+  }
+  __syncthreads();
+  rank_update(G, ldg, X, Yt, N, ldx, 2);
+  if (threadIdx.x == 0) sg[b] = (signed char)(-sg[b]);
+  __syncthreads();
+}
+
+// Global_sweep_L's trial (src/global_update.f90:228-272 with GlobalK_prop_L,
+// src/globalK.f90:115-133): the Local_sweep_L structure without observables
+// or drift statistics, the cluster's flips forced.
+__device__ __noinline__ void sweep_L_trial(const ChainDesc &c, const Smem &s, int b, double &lrf) {
+  const int N = c.N;
+  Pend pd{1, 0};
+  for (int nt = c.Ltrot; nt >= 1; --nt) {
+    if (nt % c.Nwrap == 0) { PhTimer t(c, PH_WRAP); wrap_L(c, s, nt, pd, false); }
+    scale_G_mu(c, s);                                          // propT_L
+    global_flip_slice(c, s, nt, b, lrf);
+    {
+      PhTimer t(c, PH_KIN);
+      build_table(c, s, nt);
+      kin_cols(c, s, s.G, s.ldg, N, 1);
+      kin_rows(c, s, s.G, s.ldg, N, -1);
+    }
+    if (pd.lo > pd.hi) { pd.lo = nt; pd.hi = nt; } else pd.lo = nt;
+  }
+  { PhTimer t(c, PH_WRAP); wrap_L(c, s, 0, pd, false); }
+}
+
+// Global_sweep_R's trial (src/global_update.f90:274-318, GlobalK_prop_R,
+// src/globalK.f90:135-153).
+__device__ __noinline__ void sweep_R_trial(const ChainDesc &c, const Smem &s, int b, double &lrf) {
+  const int N = c.N;
+  Pend pd{1, 0};
+  { PhTimer t(c, PH_WRAP); wrap_R(c, s, 0, pd, false); }
+  for (int nt = 1; nt <= c.Ltrot; ++nt) {
+    {
+      PhTimer t(c, PH_KIN);
+      build_table(c, s, nt);
+      kin_rows(c, s, s.G, s.ldg, N, 1);
+      kin_cols(c, s, s.G, s.ldg, N, -1);
+    }
+    global_flip_slice(c, s, nt, b, lrf);
+    if (pd.lo > pd.hi) { pd.lo = nt; pd.hi = nt; } else pd.hi = nt;
+    scale_G_mu(c, s);                                          // propT_R
+    if (nt % c.Nwrap == 0) { PhTimer t(c, PH_WRAP); wrap_R(c, s, nt, pd, false); }
+  }
+}
+
+// Global_sweep (src/global_update.f90:320-337): nglobal Wolff moves.
+__device__ __noinline__ void chain_global(const ChainDesc &c, const Smem &s, int nglobal) {
+  const int L = c.Ltrot, nb = c.nb;
+  for (int i = threadIdx.x; i < 2 * nb; i += Z2_NT) s.bond[i] = c.bonds[i];
+  __syncthreads();
+  double *gs = s.red + 40;   // [0] bond, [1] size, [2] log ratio space, [3] accept
+  int num = 0;
+  double size_sum = 0.0;
+  for (int g = 0; g < nglobal; ++g) {
+    const bool left = c.acc[A_NOTBETA] == 0.0;
+    if (threadIdx.x == 0) {
+      // Wolff_flip (src/global_update.f90:66-86) on the current sigma
+      unsigned int st = *c.rng;
+      const int b = dev_nranf(st, nb) - 1;
+      for (int t = 0; t < L; ++t) c.gmask[t] = 0;
+      int head = 0, tail = 0;
+      const int q0 = dev_nranf(st, L) - 1;
+      c.gqueue[tail++] = q0;
+      c.gmask[q0] = 1;
+      while (head < tail) {
+        const int cur = c.gqueue[head++];
+        for (int off = -1; off <= 1; off += 2) {
+          const int nbr = (cur + off + L) % L;
+          if (c.gmask[nbr]) continue;
+          if (c.sigma[(size_t)nbr * nb + b] == c.sigma[(size_t)cur * nb + b]) {
+            if (c.ptime > 0.0) {
+              st = ranf_adv(st, 1);
+              if ((double)st * (1.0 / 2147483648.0) < c.ptime) {
+                c.gqueue[tail++] = nbr;
+                c.gmask[nbr] = 1;
+              }
+            }
+          }
+        }
+      }
+      // compute_space_log_ratio (src/global_update.f90:133-172), old sigma
+      double lrs = 0.0;
+      if (c.alphaJ != 0.0) {
+        for (int t = 0; t < L; ++t) {
+          if (!c.gmask[t]) continue;
+          const signed char *sgt = c.sigma + (size_t)t * nb;
+          for (int h = 0; h < 2; ++h) {
+            double prod = (double)sgt[b];
+            for (int k = 0; k < 3; ++k) prod = prod * (double)sgt[c.bbonds[6 * b + 3 * h + k]];
+            lrs += -2.0 * c.alphaJ * prod;
+          }
+        }
+      }
+      *c.rng = st;
+      gs[0] = (double)b; gs[1] = (double)tail; gs[2] = lrs;
+    }
+    __syncthreads();
+    const int b = (int)gs[0];
+    const double size = gs[1];
+    size_sum += size;
+    global_backup(c, true);
+    load_G(c, s);
+    double lrf = 0.0;
+    if (left) sweep_L_trial(c, s, b, lrf);
+    else sweep_R_trial(c, s, b, lrf);
+    if (threadIdx.x == 0) {
+      const double lrt = lrf + gs[2];
+      unsigned int st = ranf_adv(*c.rng, 1);
+      *c.rng = st;
+      const double r = (double)st * (1.0 / 2147483648.0);
+      const bool acc = fmin(0.0, lrt) >= log(fmax(r, 1.0e-300));
+      gs[3] = acc ? 1.0 : 0.0;
+      if (acc) c.acc[A_NOTBETA] = left ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    if (gs[3] != 0.0) {
+      ++num;
+    } else {
+      // restore the state and flip the cluster back
+      global_backup(c, false);
+      for (int t = threadIdx.x; t < L; t += Z2_NT)
+        if (c.gmask[t]) {
+          signed char *p = c.sigma + (size_t)t * nb + b;
+          *p = (signed char)(-*p);
+        }
+      __syncthreads();
+    }
+  }
+  if (threadIdx.x == 0) {
+    // Acc_Kg%ratio and the cluster-size average (src/global_update.f90:330-335)
+    c.acc[A_GNUM] = (double)num;
+    c.acc[A_GDEN] = (double)nglobal;
+    if (nglobal > 0) {
+      c.acc[A_GACC] += (double)num / (double)nglobal;
+      c.acc[A_GSIZE] += size_sum / (double)nglobal;
+    }
   }
   __syncthreads();
 }

@@ -12,7 +12,8 @@
 //
 // One chain per "rank": --chains N runs N independent chains in one batch on
 // one GPU (the reference runs one per MPI rank; seeds.txt gives one seed per
-// chain).  Global moves (is_global) are not part of this path and are refused.
+// chain).  is_global runs Nglobal Wolff-in-tau moves before every bin
+// (Sweep_global%sweep, src/main.f90:76) on the GPU.
 //
 //   z2_gauge_b200 [--chains N] [--device D] [--dir PATH]
 #include <chrono>
@@ -349,10 +350,6 @@ int main(int argc, char **argv) {
     std::fprintf(stderr, "cannot read %s/paramC_sets.txt\n", dir.c_str());
     return 1;
   }
-  if (p.is_global) {
-    std::fprintf(stderr, "is_global: global moves are not part of this path\n");
-    return 1;
-  }
   if (p.Ltrot % p.Nwrap) { std::fprintf(stderr, "Ltrot must be a multiple of Nwrap\n"); return 1; }
   const int N = p.Nlx * p.Nly, nb = 2 * N;
   // initial configurations (conf_therm_in, src/fields.f90:227-309)
@@ -424,6 +421,7 @@ int main(int argc, char **argv) {
   std::vector<double> tau((size_t)7 * N * p.Ltrot), tau_sum;
   for (int nbc = 1; nbc <= p.Nbin; ++nbc) {
     const bool istau = p.is_tau && nbc > p.Nthermal;
+    if (p.is_global && (r = z2_sweep_global(h, p.Nglobal))) return fail(h, "z2_sweep_global", r);
     if ((r = z2_sweep(h, p.Nsweep, istau ? 1 : 0))) return fail(h, "z2_sweep", r);
     double mean[7] = {0};
     for (int c = 0; c < nch; ++c) {
@@ -446,6 +444,11 @@ int main(int argc, char **argv) {
       double acc = 0;
       for (int c = 0; c < nch; ++c) { double st[Z2_NSTATS]; z2_get_stats(h, c, st); acc += st[0]; }
       std::fprintf(info, " Progress %d : Accept_Klocal_shift: %.17g\n", nbc, acc / (nch * nbc));
+      if (p.is_global) {
+        double ga = 0;
+        for (int c = 0; c < nch; ++c) { double g[5]; z2_get_global_stats(h, c, g); ga += g[0]; }
+        std::fprintf(info, " Progress %d : Accept_Kglobal: %.17g\n", nbc, ga / (nch * nbc));
+      }
     }
   }
   double acc = 0, xmax = 0, xmean = 0;
@@ -456,6 +459,12 @@ int main(int argc, char **argv) {
   }
   const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   if (info) {
+    if (p.is_global) {   // Global_control_print (src/global_update.f90:339-354)
+      double ga = 0, gs = 0;
+      for (int c = 0; c < nch; ++c) { double g[5]; z2_get_global_stats(h, c, g); ga += g[0]; gs += g[1]; }
+      std::fprintf(info, " Average size of Wolff cluster : %.17g\n", gs / (nch * p.Nbin));
+      std::fprintf(info, " Accept_Kglobal                : %.17g\n", ga / (nch * p.Nbin));
+    }
     std::fprintf(info, " Accept_Klocal_shift : %.17g\n", acc / (nch * p.Nbin));
     std::fprintf(info, " Max diff Matrix     : %.17g\n", xmax);
     std::fprintf(info, " Mean diff Matrix    : %.17g\n",
