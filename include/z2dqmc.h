@@ -143,6 +143,12 @@ int z2_get_phase_cycles(const z2_handle *h, int32_t chain, double out[Z2_NPHASE]
  * call allocates a backup of each chain's state that a rejected move
  * restores.  Call after z2_pre. */
 int z2_sweep_global(z2_handle *h, int32_t nglobal);
+/* Boson-only warm-up (Local_sweep_therm, src/local_sweep.f90:73-85, and
+ * LocalK_therm, src/localK.f90:400-420; src/main.f90:38-67): nwarm sweeps of
+ * single-link Metropolis on the gauge weight alone for every chain, on the
+ * GPU.  acc (optional, [nchains]) receives each chain's mean accepted
+ * fraction (Acc_Kt%acc / nwarm).  Changes sigma: call before z2_pre. */
+int z2_therm(z2_handle *h, int32_t nwarm, double *acc);
 /* out[5]: Acc_Kg%acc (sum over calls of the accepted fraction), Wolff
  * size_cluster (sum over calls of the mean cluster size), accepted and
  * proposed moves of the last call, is_beta (1 or 0). */

@@ -451,7 +451,16 @@ static void obs_equal(Chain *c, int nt) {
 }
 
 /* ---- sweeps (src/local_sweep.f90:87-195) ---- */
+/* Local_sweep_reset (src/local_sweep.f90:63-69): for |h| <= Zero the links
+ * are made constant in tau (the value of slice 1). */
+static void reset_h0(Chain *c) {
+  if (fabs(c->h) > 1.0e-10) return;
+  for (int t = 1; t < c->Ltrot; ++t)
+    for (int b = 0; b < c->nb; ++b) c->sigma[(size_t)t * c->nb + b] = c->sigma[b];
+}
+
 static void pre(Chain *c) {
+  reset_h0(c);
   const int N = c->N;
   const size_t NN = (size_t)N * N;
   memset(c->UR, 0, NN * 8); memset(c->VR, 0, NN * 8); memset(c->UL, 0, NN * 8);
@@ -561,6 +570,7 @@ int z2cpu_run(const double *dparams, const int *iparams, double *obs, double *Go
   for (int b = 0; b < nbins; ++b) {
     c->flux_sum = c->flux_sq = c->pair = c->cdw = c->cdws = c->dens = c->nobs = 0.0;
     c->acc_num = c->acc_den = 0.0;
+    reset_h0(c);
     for (int s = 0; s < nsweep; ++s) { sweep_L(c); sweep_R(c); }
     double z = 1.0 / c->nobs, fm = c->flux_sum * z, fsq = c->flux_sq * z;
     double *o = obs + 7 * b;

@@ -1197,6 +1197,24 @@ class Z2Chain:
         if self.acc_den > 0.0:
             self.acc += self.acc_num / self.acc_den
 
+    # ---- Boson-only warm-up (src/localK.f90:400-420, src/local_sweep.f90:73-85)
+    def therm_sweep(self):
+        """``Local_sweep_therm``: one pass of ``LocalK_therm`` over (nt, ii),
+        Metropolis on the gauge weight alone; returns the accepted fraction
+        (``Acc_Kt%ratio`` adds it to ``Acc_Kt%acc``)."""
+        p = self.p
+        if abs(p.h) <= ZERO:
+            self.sigma[:, :] = self.sigma[:, :1]
+        num = 0
+        for nt in range(p.Ltrot):
+            for ii in range(2 * p.Lq):
+                s_new = -self.sigma[ii, nt]
+                ratio = boson_ratio_local(p, self.lat, self.sigma, ii, nt, s_new)
+                if ratio > self.rng():
+                    self.sigma[ii, nt] = s_new
+                    num += 1
+        return num / float(2 * p.Lq * p.Ltrot)
+
     # ---- Global Wolff-in-tau move (src/global_update.f90, src/globalK.f90) --
     def nranf(self, N: int) -> int:
         """``nranf`` (src/calc_basic.f90:113-121): nint(ranf*N + 0.5),

@@ -6,10 +6,14 @@ from oracle import z2_oracle as zo
 from oracle import z2cpu
 
 
-def test_c_port_matches_python_oracle():
-    kw = dict(RT=1.0, J=0.5, h=0.5, mu=0.1, beta=2.0, Nlx=4, Nly=4, Ltrot=20, Nwrap=5)
+import pytest
+
+
+@pytest.mark.parametrize("h", [0.5, 0.0])
+def test_c_port_matches_python_oracle(h):
+    kw = dict(RT=1.0, J=0.5, h=h, mu=0.1, beta=2.0, Nlx=4, Nly=4, Ltrot=20, Nwrap=5)
     out = z2cpu.run(**kw, seed=2024, nbins=2, record=True)
-    p = zo.Params(RT=1.0, J=0.5, h=0.5, mu=0.1, Nlx=4, Nly=4, Ltrot=20, beta=2.0, Nwrap=5)
+    p = zo.Params(RT=1.0, J=0.5, h=h, mu=0.1, Nlx=4, Nly=4, Ltrot=20, beta=2.0, Nwrap=5)
     c = zo.Z2Chain(p, seed=2024, record_decisions=True)
     c.pre()
     obs = []

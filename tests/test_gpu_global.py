@@ -59,3 +59,27 @@ def test_global_moves_match_oracle(h, mu):
             assert np.array_equal(sig, c.sigma) and iseed == c.rng.state
             assert rel(b.green(0), c.prop.Gr) < RTOL
     assert seen == {True, False}
+
+
+@pytest.mark.parametrize("h", [0.5, 0.0])
+def test_boson_warmup_matches_oracle(h):
+    """Local_sweep_therm (boson-only warm-up) on the GPU: identical
+    configuration, ranf state and accepted fraction after 3 sweeps, then a
+    bin from the warmed configuration with identical decisions."""
+    ch = Chain(RT=1.0, J=0.5, h=h, mu=0.0, Nlx=4, Nly=4, Ltrot=20, beta=2.0, Nwrap=5, seed=77)
+    c = zo.Z2Chain(_params(ch), seed=ch.seed, record_decisions=True)
+    accs = [c.therm_sweep() for _ in range(3)]
+    with Z2Batch([ch], record=True) as b:
+        acc = b.therm(3)
+        sig, iseed = b.get_config(0)
+        assert np.array_equal(sig, c.sigma)
+        assert iseed == c.rng.state
+        assert abs(acc[0] - np.mean(accs)) <= 1e-12
+        c.pre()
+        b.pre()
+        c.decisions = []
+        c.sweep()
+        b.sweep(1, False)
+        dec, _ = b.decisions(0)
+        assert np.array_equal(dec, _oracle_decisions(c, ch.Ltrot, 2 * ch.N, True))
+        assert rel(b.green(0), c.prop.Gr) < RTOL

@@ -29,7 +29,7 @@ EXPORTS = (
     "z2_get_decisions", "z2_logdet_grad", "z2_opk_mmult_R", "z2_opk_mmult_L",
     "z2_stab_UR", "z2_stab_UL", "z2_stab_green", "z2_stab_green_big",
     "z2_stab_green_noalloc", "z2_get_phase_cycles", "z2_tune_delay", "z2_get_obs_tau_k",
-    "z2_sweep_global", "z2_get_global_stats",
+    "z2_sweep_global", "z2_get_global_stats", "z2_therm",
 )
 Z2_NOALLOC_NMAX = 144
 
@@ -98,6 +98,7 @@ def load():
         "z2_stab_green_noalloc": (C.c_int, [i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp]),
         "z2_get_phase_cycles": (C.c_int, [vp, i32, dp]),
         "z2_sweep_global": (C.c_int, [vp, i32]),
+        "z2_therm": (C.c_int, [vp, i32, dp]),
         "z2_get_global_stats": (C.c_int, [vp, i32, dp]),
         "z2_tune_delay": (C.c_int, [C.POINTER(ChainParams), i32, C.POINTER(Options),
                                    C.POINTER(i32)]),

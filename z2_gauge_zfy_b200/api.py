@@ -231,6 +231,13 @@ class Z2Batch:
         a = (re + 1j * im).reshape(7, L, N)
         return {k: a[q].T.copy() for q, k in enumerate(OBS_TAU_NAMES)}
 
+    def therm(self, nwarm: int) -> np.ndarray:
+        """Boson-only warm-up of every chain (``z2_therm``); returns each
+        chain's mean accepted fraction.  Call before ``pre``."""
+        acc = np.empty(len(self.chains))
+        self._c(self.lib.z2_therm(self.h, nwarm, dptr(acc)))
+        return acc
+
     def sweep_global(self, nglobal: int):
         """Global Wolff-in-tau moves of every chain (``z2_sweep_global``,
         Sweep_global%sweep of the reference)."""

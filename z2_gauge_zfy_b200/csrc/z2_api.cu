@@ -15,7 +15,7 @@
 
 static_assert(PH_COUNT == Z2_NPHASE, "phase counters and the C ABI disagree");
 
-enum { OP_PRE = 1, OP_SWEEP = 2, OP_LOGDET = 3, OP_GLOBAL = 4 };
+enum { OP_PRE = 1, OP_SWEEP = 2, OP_LOGDET = 3, OP_GLOBAL = 4, OP_THERM = 5 };
 enum { U_MMULT_R = 1, U_MMULT_L, U_STAB_UR, U_STAB_UL, U_STAB_GREEN, U_STAB_GREEN_BIG };
 
 struct UnitArgs {
@@ -63,6 +63,8 @@ z2_chain_kernel(const ChainDesc *descs, const int *order, int nchains, int *queu
       chain_logdet_grad(sc, s);
     } else if (op == OP_GLOBAL) {
       chain_global(sc, s, nsweep);
+    } else if (op == OP_THERM) {
+      chain_therm(sc, s, nsweep);
     }
     __syncthreads();
   }
@@ -804,6 +806,28 @@ extern "C" int z2_get_obs_tau_k(const z2_handle *h, int32_t chain, double *re, d
 }
 
 static int upload_desc(z2_handle *h, int chain);
+
+// Boson-only warm-up of every chain (Local_sweep_therm, src/main.f90:38-67):
+// nwarm sweeps of LocalK_therm; acc (optional, [nchains]) receives each
+// chain's Acc_Kt%acc / nwarm.  Changes sigma, so z2_pre must follow.
+extern "C" int z2_therm(z2_handle *h, int32_t nwarm, double *acc) {
+  if (!h) return Z2_ERR_ARG;
+  if (nwarm < 0) return set_err(h, Z2_ERR_ARG, "z2_therm: nwarm = %d", nwarm);
+  if (nwarm > 0) {
+    int r = launch_chains(h, OP_THERM, nwarm, 0, nullptr);
+    if (r) return r;
+  }
+  h->pre_done = false;
+  if (acc) {
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    for (int c = 0; c < h->nchains; ++c) {
+      double a = 0.0;
+      CUDA_TRY(h, cudaMemcpy(&a, h->ch[c].d.acc + A_TACC, sizeof(double), cudaMemcpyDeviceToHost));
+      acc[c] = nwarm > 0 ? a / nwarm : 0.0;
+    }
+  }
+  return Z2_OK;
+}
 
 // Global_sweep for every chain (src/global_update.f90:320-337).  The backup
 // of the chain state that a rejected move restores is allocated on the first

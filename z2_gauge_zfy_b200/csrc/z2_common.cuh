@@ -25,6 +25,7 @@ enum {
   // Global_sweep, Acc_Kg%acc, Wolff%size_cluster, sweep direction (0: the
   // next bin runs L then R, the reference's is_beta = .true.)
   A_GNUM, A_GDEN, A_GACC, A_GSIZE, A_NOTBETA,
+  A_TACC,                        // Acc_Kt%acc of the boson-only warm-up
   A_PH0,                         // Z2_NPHASE per-phase SM cycle counters
   A_COUNT = A_PH0 + 12
 };

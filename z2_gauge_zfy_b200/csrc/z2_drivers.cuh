@@ -76,6 +76,13 @@ __device__ __noinline__ void dyn_sweep(const ChainDesc &c, const Smem &s) {
 __device__ __noinline__ void chain_pre(const ChainDesc &c, const Smem &s) {
   const int N = c.N;
   if (threadIdx.x == 0) c.acc[A_NOTBETA] = 0.0;   // is_beta = .true. (src/main.f90:73)
+  if (c.hzero) {   // this%reset (src/local_sweep.f90:63-69): sigma constant in tau
+    for (int b = threadIdx.x; b < c.nb; b += Z2_NT) {
+      const signed char v = c.sigma[b];
+      for (int t = 1; t < c.Ltrot; ++t) c.sigma[(size_t)t * c.nb + b] = v;
+    }
+    __syncthreads();
+  }
   blk_identity(c.UR, N, N); blk_identity(c.VR, N, N); blk_fill(c.DR, N, 1.0);
   blk_identity(c.ULT, N, N); blk_identity(c.VL, N, N); blk_fill(c.DL, N, 1.0);
   blk_identity(c.G, N, N);
@@ -194,6 +201,62 @@ __device__ __noinline__ void chain_sweep(const ChainDesc &c, const Smem &s, int 
     const double z = 1.0 / c.acc[A_NOBST];
     const size_t n = (size_t)7 * c.Ltrot * N;
     for (size_t i = threadIdx.x; i < n; i += Z2_NT) c.obs_tau[i] = z * c.obs_tau[i];
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// Boson-only warm-up: Local_sweep_therm (src/local_sweep.f90:73-85) with
+// LocalK_therm (src/localK.f90:400-420), Metropolis on the gauge weight alone.
+// The sweep is one ordered pass of ranf draws, so thread 0 runs it, on the
+// configuration staged in shared memory when it fits (the arena is free
+// before z2_pre).  Acc_Kt%acc accumulates in A_TACC.
+// ---------------------------------------------------------------------------
+__device__ __noinline__ void chain_therm(const ChainDesc &c, const Smem &s, int nwarm) {
+  const int L = c.Ltrot, nb = c.nb;
+  const size_t bytes = (size_t)L * nb;
+  const size_t arena = 8 * ((c.g_in_smem ? (size_t)c.N * s.ldg : 0) + (size_t)s.tile_doubles);
+  const bool staged = bytes <= arena;
+  signed char *sig = staged ? reinterpret_cast<signed char *>(s.arena) : c.sigma;
+  if (staged) {
+    for (size_t i = threadIdx.x; i < bytes; i += Z2_NT) sig[i] = c.sigma[i];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned int st = *c.rng;
+    double acc = 0.0;
+    for (int w = 0; w < nwarm; ++w) {
+      if (c.hzero)   // Local_sweep_reset (src/local_sweep.f90:63-66)
+        for (int t = 1; t < L; ++t)
+          for (int b = 0; b < nb; ++b) sig[(size_t)t * nb + b] = sig[b];
+      int num = 0;
+      for (int t = 0; t < L; ++t) {
+        signed char *sg = sig + (size_t)t * nb;
+        const signed char *sp = sig + (size_t)((t - 1 + L) % L) * nb;
+        const signed char *sn = sig + (size_t)((t + 1) % L) * nb;
+        for (int b = 0; b < nb; ++b) {
+          const int *bb = c.bbonds + 6 * b;
+          const double s_old = (double)sg[b];
+          const double tmp_old = s_old * sg[bb[0]] * sg[bb[1]] * sg[bb[2]] +
+                                 s_old * sg[bb[3]] * sg[bb[4]] * sg[bb[5]];
+          const int is = (int)(-2.0 * tmp_old + 4.0) >> 2;
+          const double tn = s_old * ((double)sp[b] + (double)sn[b]);
+          const int it = (int)(-2.0 * tn + 4.0) >> 2;
+          st = ranf_adv(st, 1);
+          if (c.rb[is * 3 + it] > (double)st * (1.0 / 2147483648.0)) {
+            sg[b] = (signed char)(-sg[b]);
+            ++num;
+          }
+        }
+      }
+      acc += (double)num / (double)((size_t)nb * L);
+    }
+    *c.rng = st;
+    c.acc[A_TACC] += acc;
+  }
+  __syncthreads();
+  if (staged) {
+    for (size_t i = threadIdx.x; i < bytes; i += Z2_NT) c.sigma[i] = sig[i];
   }
   __syncthreads();
 }
