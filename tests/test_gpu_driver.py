@@ -140,3 +140,27 @@ def test_driver_global_moves(tmp_path):
         assert np.allclose(got, np.array(v), rtol=1e-10, atol=1e-12), k
     info = (tmp_path / "info.txt").read_text()
     assert "Accept_Kglobal" in info and "Wolff cluster" in info
+
+
+def test_driver_warm_up(tmp_path):
+    """is_warm: Nwarm boson-only sweeps (Local_sweep_therm, src/main.f90:38-67)
+    on the GPU before Local_sweep_pre, then per-bin observables against the
+    oracle doing the same."""
+    build.build()
+    params = PARAMS.replace(".false. 0\n.false. 0\n.false. 0\n", ".false. 0\n.true. 3\n.false. 0\n")
+    (tmp_path / "paramC_sets.txt").write_text(params)
+    (tmp_path / "confin.txt").write_text("0\n")
+    (tmp_path / "seeds.txt").write_text("12345\n")
+    r = subprocess.run([build.DRIVER, "--chains", "1", "--dir", str(tmp_path)],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    p = zo.read_params(str(tmp_path / "paramC_sets.txt"))
+    assert p.is_warm and p.Nwarm == 3
+    c = zo.Z2Chain(p, seed=12345)
+    for _ in range(p.Nwarm):
+        c.therm_sweep()
+    c.pre()
+    ref = _oracle_bins(p, [c])
+    for k in ref:
+        got = np.array([float(x) for x in (tmp_path / k).read_text().split()])
+        assert np.allclose(got, ref[k], rtol=1e-10, atol=1e-12), k

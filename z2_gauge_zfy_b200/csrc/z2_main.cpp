@@ -4,7 +4,7 @@
 //   paramC_sets.txt  (read_input, src/calc_basic.f90:50-89)
 //   confin.txt / seeds.txt -> sigma (conf_therm_in + conf_set + conf_transfer,
 //                                    src/fields.f90:214-507)
-//   optional boson-only warm-up (LocalK_therm, src/localK.f90:400-420)
+//   optional boson-only warm-up (LocalK_therm, src/localK.f90:400-420) on the GPU
 //   Sweep_local%pre, then Nbin bins of Sweep_local%sweep (src/main.f90:72-103)
 //   per bin: flux_avg, chi_flux, pair_sc_q0, cdw_pi, cdw_ratio, density
 //            appended, averaged over chains (Fourier%preq, src/fourier_trans.f90:251-315)
@@ -130,69 +130,6 @@ std::vector<double> conf_transfer(const Params &p, const std::vector<double> &st
     for (int b = 0; b < nb; ++b) s[(size_t)nt * nb + b] = s[(size_t)(nt - p.LtrotT) * nb + b];
   return s;
 }
-
-// LocalK_therm sweep on the host (src/localK.f90:400-420, src/local_sweep.f90:73-85).
-struct Warm {
-  int Lx, Ly, N, nb, Lt;
-  std::vector<int> bb;   // [nb][6] plaquette partners (src/lattice.f90:104-141)
-  double rb[9];
-  explicit Warm(const Params &p) : Lx(p.Nlx), Ly(p.Nly), N(p.Nlx * p.Nly), nb(2 * N), Lt(p.Ltrot) {
-    auto site = [&](int x, int y) { return (y - 1) * Lx + (x - 1); };
-    auto bond = [&](int a, int b2) -> int {   // inv_bond_list
-      int ax = a % Lx + 1, ay = a / Lx + 1;
-      if (site(npbc(ax + 1, Lx), ay) == b2) return 2 * a;
-      return 2 * a + 1;
-    };
-    bb.assign(6 * nb, 0);
-    for (int nc = 0; nc < nb; ++nc) {
-      int ii = nc / 2, ix = ii % Lx + 1, iy = ii / Lx + 1;
-      int *o = &bb[6 * nc];
-      if (nc % 2 == 0) {
-        int jj = site(npbc(ix + 1, Lx), iy), jx = jj % Lx + 1, jy = jj / Lx + 1;
-        int nx = site(ix, npbc(iy + 1, Ly)); o[0] = bond(ii, nx);
-        int ny = site(jx, npbc(jy + 1, Ly)); o[1] = bond(nx, ny); o[2] = bond(jj, ny);
-        nx = site(ix, npbc(iy - 1, Ly)); o[3] = bond(nx, ii);
-        ny = site(jx, npbc(jy - 1, Ly)); o[4] = bond(nx, ny); o[5] = bond(ny, jj);
-      } else {
-        int jj = site(ix, npbc(iy + 1, Ly)), jx = jj % Lx + 1, jy = jj / Lx + 1;
-        int nx = site(npbc(jx - 1, Lx), jy); o[0] = bond(nx, jj);
-        int ny = site(npbc(ix - 1, Lx), iy); o[1] = bond(ny, nx); o[2] = bond(ny, ii);
-        nx = site(npbc(jx + 1, Lx), jy); o[3] = bond(jj, nx);
-        ny = site(npbc(ix + 1, Lx), iy); o[4] = bond(ny, nx); o[5] = bond(ii, ny);
-      }
-    }
-    const double dtau = p.beta / p.Ltrot, alpha = dtau * p.J, lub = std::log(1.0e200);
-    double gamma = 0.0; bool temporal = false;
-    if (std::fabs(p.h) > 1.0e-10) {
-      double ta = std::tanh(dtau * p.h);
-      if (ta < 1.0e-300) ta = 1.0e-300;
-      gamma = -0.5 * std::log(ta); temporal = true;
-    }
-    for (int is = 0; is < 3; ++is)
-      for (int it = 0; it < 3; ++it) {
-        double e = std::min(std::max(alpha * (4.0 * is - 4.0), -lub), lub), r = std::exp(e);
-        if (temporal) r = r * std::exp(std::min(std::max(gamma * (4.0 * it - 4.0), -lub), lub));
-        rb[is * 3 + it] = r;
-      }
-  }
-  // one therm sweep; returns accepted count
-  int sweep(std::vector<double> &s, uint32_t &iq) const {
-    int acc = 0;
-    for (int nt = 0; nt < Lt; ++nt) {
-      double *sg = &s[(size_t)nt * nb];
-      const double *sp = &s[(size_t)((nt - 1 + Lt) % Lt) * nb], *sn = &s[(size_t)((nt + 1) % Lt) * nb];
-      for (int b = 0; b < nb; ++b) {
-        const int *o = &bb[6 * b];
-        double so = sg[b];
-        double to = so * sg[o[0]] * sg[o[1]] * sg[o[2]] + so * sg[o[3]] * sg[o[4]] * sg[o[5]];
-        int is = (int)(-2.0 * to + 4.0) >> 2;
-        int it = (int)(-2.0 * so * (sp[b] + sn[b]) + 4.0) >> 2;
-        if (rb[is * 3 + it] > ranf(iq)) { sg[b] = -so; ++acc; }
-      }
-    }
-    return acc;
-  }
-};
 
 void append(const std::string &dir, const char *name, double v) {
   FILE *f = std::fopen((dir + "/" + name).c_str(), "a");
@@ -393,14 +330,6 @@ int main(int argc, char **argv) {
                  p.beta, p.Ltrot, p.beta / p.Ltrot, p.Nwrap, p.Nbin, p.Nsweep, nch);
     std::fprintf(info, " ==============================================\n");
   }
-  // boson warm-up on the host
-  if (p.is_warm && p.Nwarm > 0) {
-    Warm w(p);
-    double acc = 0.0;
-    for (int c = 0; c < nch; ++c)
-      for (int n = 0; n < p.Nwarm; ++n) acc += w.sweep(sig[c], iseed[c]) / double(nb * p.Ltrot);
-    if (info) std::fprintf(info, " Thermalize Accept Ratio : %.17g\n", acc / (nch * p.Nwarm));
-  }
   std::vector<z2_chain_params> cp(nch);
   for (int c = 0; c < nch; ++c)
     cp[c] = z2_chain_params{p.RT, p.J, p.h, p.mu, p.Q, p.Nlx, p.Nly, p.Ltrot, p.beta,
@@ -416,6 +345,14 @@ int main(int argc, char **argv) {
   if (r) return fail(h, "z2_create", r);
   for (int c = 0; c < nch; ++c)
     if ((r = z2_set_config(h, c, sig[c].data(), (int32_t)iseed[c]))) return fail(h, "z2_set_config", r);
+  // boson-only warm-up on the GPU (src/main.f90:38-67)
+  if (p.is_warm && p.Nwarm > 0) {
+    std::vector<double> wacc(nch, 0.0);
+    if ((r = z2_therm(h, p.Nwarm, wacc.data()))) return fail(h, "z2_therm", r);
+    double acc = 0.0;
+    for (double a : wacc) acc += a / nch;
+    if (info) std::fprintf(info, " Thermalize Accept Ratio : %.17g\n", acc);
+  }
   if ((r = z2_pre(h))) return fail(h, "z2_pre", r);
   const char *names[7] = {"flux_avg", "chi_flux", "pair_sc_q0", "cdw_pi", "cdw_shift", "cdw_ratio", "density"};
   std::vector<double> tau((size_t)7 * N * p.Ltrot), tau_sum;
