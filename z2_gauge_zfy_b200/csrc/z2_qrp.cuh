@@ -9,14 +9,18 @@
 // never touches shared memory.  The norm downdate of a column group runs on S
 // lanes of its half-warp at once.  A step costs two block barriers: one after
 // the reflector of the pivot column is published, one after the per-warp
-// pivot candidates are published.
+// pivot candidates are published.  The reflector is on every step's critical
+// path (the other warps wait for it), so its warp extracts the pivot column
+// with a jump to a static copy, forms |beta| with one square root, and writes
+// the finished column straight to its final place in A.
 //
 // Pivoting follows DGEQP3 without moving data: the logical position of every
 // physical column is tracked (pos / lp2c), the arg-max breaks ties by logical
 // position as IDAMAX does on the swapped arrays, and the partial norm
-// downdate and its recompute threshold are DLAQP2's.  The factors are written
-// back in logical column order at the end, so the result has DGEQP3's layout
-// (R above the diagonal, reflectors below, tau, 1-based jpvt).
+// downdate and its recompute threshold are DLAQP2's.  Each column is written
+// to A at the step that factors it, at its logical position, so the result
+// has DGEQP3's layout (R above the diagonal, reflectors below, tau, 1-based
+// jpvt).
 #pragma once
 #include "z2_dmma.cuh"
 
@@ -28,10 +32,68 @@ __device__ __forceinline__ double hw_sum(double v) {
   return v;
 }
 
-// better pivot candidate: larger norm, then smaller logical position
-__device__ __forceinline__ bool qrp_better(double v, int p, double bv, int bp) {
-  return v > bv || (v == bv && p < bp);
+// Arg-max over the 32 lanes of a warp of (v, p): larger v, then smaller p.
+// v is a column norm (>= 0) or negative for "no candidate" (p = INT_MAX).
+// Non-negative doubles order like their bit patterns, so the key is the
+// 64-bit pattern (0 for v <= 0 or NaN, where the ordering only has to put
+// every real candidate ahead of the empty lanes) and the reduction is three
+// warp reductions (high word, low word, position) instead of a five-level
+// shuffle butterfly over three values.
+__device__ __forceinline__ void warp_argmax_vp(double v, int p, double &bv, int &bp) {
+  const unsigned long long key = (v > 0.0) ? (unsigned long long)__double_as_longlong(v) : 0ull;
+  const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+  const unsigned mhi = __reduce_max_sync(Z2_FULL, hi);
+  const unsigned mlo = __reduce_max_sync(Z2_FULL, hi == mhi ? lo : 0u);
+  const bool cand = hi == mhi && lo == mlo;
+  const unsigned mp = __reduce_min_sync(Z2_FULL, cand ? (unsigned)p : 0xffffffffu);
+  bp = (int)mp;
+  bv = (mp >= 0x7fffffffu) ? -1.0
+                           : __longlong_as_double((long long)(((unsigned long long)mhi << 32) | mlo));
 }
+
+// The per-step pivot: every warp reduces the eight warp candidates (lanes
+// 0..7) the same way and takes the winner's physical column from widx
+// (logical positions are unique, so the winning warp is the one whose wpos
+// matches).
+__device__ __forceinline__ int block_pivot(const double *wmax, const int *wpos, const int *widx) {
+  const int lane = threadIdx.x & 31;
+  const double v = lane < Z2_WARPS ? wmax[lane] : -1.0;
+  const int p = lane < Z2_WARPS ? wpos[lane] : 0x7fffffff;
+  const int c = lane < Z2_WARPS ? widx[lane] : 0;
+  double bv; int bp;
+  warp_argmax_vp(v, p, bv, bp);
+  const unsigned w = __ballot_sync(Z2_FULL, lane < Z2_WARPS && p == bp);
+  return __shfl_sync(Z2_FULL, c, w ? __ffs(w) - 1 : 0);
+}
+
+// Static-index views of the register tile: a[.][q] / a[p][.] for a warp-
+// uniform runtime q or p, as a jump into one of S straight copies (a
+// predicated select over all S x S registers costs S times more issue).
+#define QRP_CASE_COL(Q) \
+  case Q:               \
+    if (Q < S) {        \
+      _Pragma("unroll") for (int p = 0; p < S; ++p) col[p] = a[p][Q < S ? Q : 0]; \
+    }                   \
+    break;
+#define QRP_CASE_ROW(P) \
+  case P:               \
+    if (P < S) {        \
+      _Pragma("unroll") for (int q = 0; q < S; ++q) rowj[q] = a[P < S ? P : 0][q]; \
+    }                   \
+    break;
+// Row blocks above the current step are zero in the reflector: the dot
+// products and the rank-1 update enter their unrolled sequences at block pj
+// (fall-through switch).
+#define QRP_CASE_DOT(P) \
+  case P:               \
+    if (P < S) {        \
+      _Pragma("unroll") for (int q = 0; q < S; ++q) d[q] += vr[P < S ? P : 0] * a[P < S ? P : 0][q]; \
+    }
+#define QRP_CASE_UPD(P) \
+  case P:               \
+    if (P < S) {        \
+      _Pragma("unroll") for (int q = 0; q < S; ++q) a[P < S ? P : 0][q] -= d[q] * vr[P < S ? P : 0]; \
+    }
 
 // work: >= 2 n doubles (reflector + two int maps); red: >= 32 doubles.
 template <int S>
@@ -87,77 +149,70 @@ __device__ __noinline__ void qrp_reg(double *A, int lda, int n, int *jpvt, doubl
   __syncthreads();
   int pc;
   {
-    // pivot of step 0
-    double bv = -1.0; int bp = 0x7fffffff, bc = -1;
-    for (int c = tid; c < n; c += Z2_NT)
-      if (qrp_better(vn1[c], c, bv, bp)) { bv = vn1[c]; bp = c; bc = c; }
-#pragma unroll
-    for (int o = 16; o; o >>= 1) {
-      const double ov = __shfl_xor_sync(Z2_FULL, bv, o);
-      const int op = __shfl_xor_sync(Z2_FULL, bp, o), oc = __shfl_xor_sync(Z2_FULL, bc, o);
-      if (qrp_better(ov, op, bv, bp)) { bv = ov; bp = op; bc = oc; }
+    // pivot of step 0 (physical = logical order)
+    double bv = -1.0; int bp = 0x7fffffff;
+    for (int c = lane; c < n; c += 32) {
+      const double v = vn1[c];
+      if (v > bv || (v == bv && c < bp)) { bv = v; bp = c; }
     }
-    if (lane == 0) { wmax[warp] = bv; wpos[warp] = bp; widx[warp] = bc; }
-    __syncthreads();
-    bv = wmax[0]; bp = wpos[0]; bc = widx[0];
-#pragma unroll
-    for (int w = 1; w < Z2_WARPS; ++w)
-      if (qrp_better(wmax[w], wpos[w], bv, bp)) { bv = wmax[w]; bp = wpos[w]; bc = widx[w]; }
-    pc = bc;
-    __syncthreads();
+    double wv; int wp;
+    warp_argmax_vp(bv, bp, wv, wp);
+    pc = wp;   // every warp scans all columns: no block step
   }
 
   for (int j = 0; j < n; ++j) {
     const int qc = pc >> 4, gc = pc & 15;
     const int pj = j >> 4, oj = j & 15;
-    // ---- reflector of the pivot column (DLARFG), by the warp holding it ----
+    // ---- reflector of the pivot column (DLARFG), by the warp holding it.
+    // The finished column (R above the diagonal, beta, v below) goes straight
+    // to its final place A(:, j); its registers are not used again. ----
     if (warp == (gc >> 1)) {
       const bool mine = (lane >> 4) == (gc & 1);
       double col[S];
 #pragma unroll
       for (int p = 0; p < S; ++p) col[p] = 0.0;
-#pragma unroll
-      for (int q = 0; q < S; ++q)
-        if (q == qc) {
-#pragma unroll
-          for (int p = 0; p < S; ++p) col[p] = a[p][q];
-        }
-      double ss = 0.0, aj = 0.0;
+      switch (qc) {
+        QRP_CASE_COL(0) QRP_CASE_COL(1) QRP_CASE_COL(2) QRP_CASE_COL(3) QRP_CASE_COL(4)
+        QRP_CASE_COL(5) QRP_CASE_COL(6) QRP_CASE_COL(7) QRP_CASE_COL(8)
+        default: break;
+      }
+      double s0 = 0.0, s1 = 0.0, aj = 0.0;
 #pragma unroll
       for (int p = 0; p < S; ++p) {
         const int r = tr + 16 * p;
-        if (r > j && r < n) ss += col[p] * col[p];
+        const double x = (r > j && r < n) ? col[p] : 0.0;
+        if (p & 1) s1 += x * x; else s0 += x * x;
         if (p == pj) aj = col[p];
       }
-      ss = hw_sum(ss);
+      const double ss = hw_sum(s0 + s1);
       const double alpha = __shfl_sync(Z2_FULL, aj, hl | oj);
       double t = 0.0, beta = alpha, sc = 1.0;
       if (j < n - 1 && ss != 0.0) {
-        const double xnorm = sqrt(ss);
-        beta = -copysign(dlapy2(alpha, xnorm), alpha);
+        // |beta| = sqrt(alpha^2 + xnorm^2) (DLAPY2 without its rescaling,
+        // which only matters past the overflow threshold: kept as fallback)
+        double nb = sqrt(fma(alpha, alpha, ss));
+        if (isinf(nb)) nb = dlapy2(alpha, sqrt(ss));
+        beta = -copysign(nb, alpha);
         t = (beta - alpha) / beta;
         sc = 1.0 / (alpha - beta);
       }
-#pragma unroll
-      for (int p = 0; p < S; ++p) {
-        const int r = tr + 16 * p;
-        double vv = 0.0;
-        if (r > j) {
-          if (t != 0.0) col[p] *= sc;
-          vv = col[p];
-        } else if (r == j) {
-          col[p] = beta;
-          vv = 1.0;
-        }
-        if (mine && r < n) vsh[r] = vv;
-      }
       if (mine) {
 #pragma unroll
-        for (int q = 0; q < S; ++q)
-          if (q == qc) {
-#pragma unroll
-            for (int p = 0; p < S; ++p) a[p][q] = col[p];
+        for (int p = 0; p < S; ++p) {
+          const int r = tr + 16 * p;
+          double vv = 0.0, out = col[p];
+          if (r > j) {
+            if (t != 0.0) out *= sc;
+            vv = out;
+          } else if (r == j) {
+            out = beta;
+            vv = 1.0;
           }
+          if (r < n) {
+            vsh[r] = vv;
+            A[r + (size_t)j * lda] = out;
+          }
+        }
         if (tr == 0) { *tsh = t; tau[j] = t; }
       }
     }
@@ -177,34 +232,36 @@ __device__ __noinline__ void qrp_reg(double *A, int lda, int n, int *jpvt, doubl
       for (int p = 0; p < S; ++p) {
         const int r = tr + 16 * p;
         vr[p] = (r < n) ? vsh[r] : 0.0;   // 0 above row j
+        d[p] = 0.0;
+      }
+      switch (pj) {
+        QRP_CASE_DOT(0) QRP_CASE_DOT(1) QRP_CASE_DOT(2) QRP_CASE_DOT(3) QRP_CASE_DOT(4)
+        QRP_CASE_DOT(5) QRP_CASE_DOT(6) QRP_CASE_DOT(7) QRP_CASE_DOT(8)
+        default: break;
       }
 #pragma unroll
-      for (int q = 0; q < S; ++q) {
-        double s0 = 0.0;
+      for (int o = 8; o; o >>= 1) {
 #pragma unroll
-        for (int p = 0; p < S; ++p) s0 += vr[p] * a[p][q];
-        d[q] = s0;
+        for (int q = 0; q < S; ++q) d[q] += __shfl_xor_sync(Z2_FULL, d[q], o);
       }
-#pragma unroll
-      for (int q = 0; q < S; ++q) d[q] = hw_sum(d[q]);
 #pragma unroll
       for (int q = 0; q < S; ++q) d[q] = ((done >> q) & 1u) ? 0.0 : t * d[q];
-#pragma unroll
-      for (int p = 0; p < S; ++p)
-#pragma unroll
-        for (int q = 0; q < S; ++q) a[p][q] -= d[q] * vr[p];
+      switch (pj) {
+        QRP_CASE_UPD(0) QRP_CASE_UPD(1) QRP_CASE_UPD(2) QRP_CASE_UPD(3) QRP_CASE_UPD(4)
+        QRP_CASE_UPD(5) QRP_CASE_UPD(6) QRP_CASE_UPD(7) QRP_CASE_UPD(8)
+        default: break;
+      }
     }
     // ---- partial norm downdate (DLAQP2): lane q of each half-warp takes
     // column slot q; row j of the group comes from its owner lane ----
     double rowj[S];
 #pragma unroll
     for (int q = 0; q < S; ++q) rowj[q] = 0.0;
-#pragma unroll
-    for (int p = 0; p < S; ++p)
-      if (p == pj) {
-#pragma unroll
-        for (int q = 0; q < S; ++q) rowj[q] = a[p][q];
-      }
+    switch (pj) {
+      QRP_CASE_ROW(0) QRP_CASE_ROW(1) QRP_CASE_ROW(2) QRP_CASE_ROW(3) QRP_CASE_ROW(4)
+      QRP_CASE_ROW(5) QRP_CASE_ROW(6) QRP_CASE_ROW(7) QRP_CASE_ROW(8)
+      default: break;
+    }
     double ajc = 0.0;
 #pragma unroll
     for (int q = 0; q < S; ++q) {
@@ -219,9 +276,9 @@ __device__ __noinline__ void qrp_reg(double *A, int lda, int n, int *jpvt, doubl
       v1 = vn1[cq];
       if (v1 != 0.0) {
         double temp = fabs(ajc) / v1;
+        const double qq = v1 / vn2[cq];
         temp = 1.0 - temp * temp;
         temp = fmax(temp, 0.0);
-        const double qq = v1 / vn2[cq];
         if (temp * qq * qq <= tol3z) {
           need = true;
         } else {
@@ -251,38 +308,26 @@ __device__ __noinline__ void qrp_reg(double *A, int lda, int n, int *jpvt, doubl
         }
       }
     }
-    // ---- pivot candidate of this warp ----
-    double bv = -1.0; int bp = 0x7fffffff, bc = -1;
-    if (act) { bv = v1; bp = pos[cq]; bc = cq; }
-#pragma unroll
-    for (int o = 16; o; o >>= 1) {
-      const double ov = __shfl_xor_sync(Z2_FULL, bv, o);
-      const int op = __shfl_xor_sync(Z2_FULL, bp, o), oc = __shfl_xor_sync(Z2_FULL, bc, o);
-      if (qrp_better(ov, op, bv, bp)) { bv = ov; bp = op; bc = oc; }
+    // ---- pivot candidate of this warp, then of the block ----
+    double bv; int bp;
+    warp_argmax_vp(act ? v1 : -1.0, act ? pos[cq] : 0x7fffffff, bv, bp);
+    if (lane == 0) {
+      // lp2c changes next only after the barrier below (the next swap)
+      wmax[warp] = bv; wpos[warp] = bp; widx[warp] = (bp < n) ? lp2c[bp] : 0;
     }
-    if (lane == 0) { wmax[warp] = bv; wpos[warp] = bp; widx[warp] = bc; }
     __syncthreads();
-    if (j + 1 < n) {
-      bv = wmax[0]; bp = wpos[0]; bc = widx[0];
-#pragma unroll
-      for (int w = 1; w < Z2_WARPS; ++w)
-        if (qrp_better(wmax[w], wpos[w], bv, bp)) { bv = wmax[w]; bp = wpos[w]; bc = widx[w]; }
-      pc = bc;
-    }
+    if (j + 1 < n) pc = block_pivot(wmax, wpos, widx);
     // no barrier here: wmax, vsh, tsh and pos are written again only after
-    // the next step's first barrier, which every reader passes after its reads
+    // the next step's first barrier, which every reader passes after its
+    // reads
   }
-  // write back in logical column order
-#pragma unroll
-  for (int p = 0; p < S; ++p)
-#pragma unroll
-    for (int q = 0; q < S; ++q) {
-      const int r = tr + 16 * p, c = tc + 16 * q;
-      if (r < n && c < n) A[r + (size_t)pos[c] * lda] = a[p][q];
-    }
   for (int l = tid; l < n; l += Z2_NT) jpvt[l] = lp2c[l] + 1;
   __syncthreads();
 }
+#undef QRP_CASE_COL
+#undef QRP_CASE_ROW
+#undef QRP_CASE_DOT
+#undef QRP_CASE_UPD
 
 // Pivoted QR of the stabilization: register-resident for n <= 144, the
 // thread-per-column kernel above that (or without 2n doubles of work space).
