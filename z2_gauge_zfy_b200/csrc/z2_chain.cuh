@@ -297,10 +297,77 @@ __device__ __noinline__ void green_big_extract(int N, const double *B3, double *
 // ---------------------------------------------------------------------------
 // Delayed rank-2 updates (LocalK_metro, src/localK.f90:45-173)
 // ---------------------------------------------------------------------------
+// G <- G - X Yt^T over the m queued columns (ld ldx) when 8 TR and 8 TC
+// divide N: each warp owns (8 TR) x (8 TC) blocks of G, reads their old
+// values before its DMMA chain (the load latency overlaps the products) and
+// reuses each X fragment TC times and each Yt fragment TR times.  The k loop
+// and the final -acc + old are those of blk_dmma, so the result is the same
+// to the bit.
+template <int TR, int TC>
+__device__ __noinline__ void flush_tiles(double *G, int ldg, const double *X, const double *Yt,
+                                         int N, int ldx, int m) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int lr = lane >> 2, lc = lane & 3;
+  const int gr = N / (8 * TR), gcn = N / (8 * TC);
+  const int m4 = m & ~3;
+  const size_t s4 = (size_t)4 * ldx;
+  for (int g = warp; g < gr * gcn; g += Z2_WARPS) {
+    const int r0 = (g % gr) * 8 * TR, c0 = (g / gr) * 8 * TC;
+    double *cp = G + r0 + lr + (size_t)(c0 + 2 * lc) * ldg;
+    double old[TR][TC][2], acc[TR][TC][2];
+#pragma unroll
+    for (int a = 0; a < TR; ++a)
+#pragma unroll
+      for (int b = 0; b < TC; ++b)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          old[a][b][e] = cp[8 * a + (size_t)(8 * b + e) * ldg];
+          acc[a][b][e] = 0.0;
+        }
+    const double *pa = X + r0 + lr + (size_t)lc * ldx;
+    const double *pb = Yt + c0 + lr + (size_t)lc * ldx;
+#pragma unroll 2
+    for (int l0 = 0; l0 < m4; l0 += 4) {
+      double fa[TR], fb[TC];
+#pragma unroll
+      for (int u = 0; u < TR; ++u) fa[u] = pa[8 * u];
+#pragma unroll
+      for (int v = 0; v < TC; ++v) fb[v] = pb[8 * v];
+      pa += s4; pb += s4;
+#pragma unroll
+      for (int u = 0; u < TR; ++u)
+#pragma unroll
+        for (int v = 0; v < TC; ++v) dmma884(acc[u][v][0], acc[u][v][1], fa[u], fb[v]);
+    }
+    if (m4 < m) {
+      // two trailing columns: lanes lc >= m - m4 feed zeros
+      const bool ok = lc < m - m4;
+      double fa[TR], fb[TC];
+#pragma unroll
+      for (int u = 0; u < TR; ++u) fa[u] = ok ? pa[8 * u] : 0.0;
+#pragma unroll
+      for (int v = 0; v < TC; ++v) fb[v] = ok ? pb[8 * v] : 0.0;
+#pragma unroll
+      for (int u = 0; u < TR; ++u)
+#pragma unroll
+        for (int v = 0; v < TC; ++v) dmma884(acc[u][v][0], acc[u][v][1], fa[u], fb[v]);
+    }
+#pragma unroll
+    for (int a = 0; a < TR; ++a)
+#pragma unroll
+      for (int b = 0; b < TC; ++b)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) cp[8 * a + (size_t)(8 * b + e) * ldg] = -acc[a][b][e] + old[a][b][e];
+  }
+  __syncthreads();
+}
+
 // G <- G - X Yt^T over the m queued columns (ld ldx): one DMMA rank-m update.
 __device__ __forceinline__ void rank_update(double *G, int ldg, const double *X, const double *Yt,
                                             int N, int ldx, int m) {
-  blk_dmma(N, N, m, -1.0, MatRef{X, 1, ldx}, false, MatRef{Yt, ldx, 1}, false, 1.0, G, ldg);
+  if (N % 24 == 0) flush_tiles<3, 3>(G, ldg, X, Yt, N, ldx, m);
+  else if (N % 16 == 0) flush_tiles<2, 2>(G, ldg, X, Yt, N, ldx, m);
+  else blk_dmma(N, N, m, -1.0, MatRef{X, 1, ldx}, false, MatRef{Yt, ldx, 1}, false, 1.0, G, ldg);
 }
 
 // The 2N proposals of one slice (LocalK_prop_L: bonds 2N..1, LocalK_prop_R:

@@ -112,7 +112,7 @@ struct Smem {
   double *G;        // G (smem arena or global)
   int ldg;          // leading dimension of G
   double *X, *Yt;   // delayed-update factors [k2][ldx]
-  int ldx;          // odd leading dimension of X, Yt
+  int ldx;          // leading dimension of X, Yt (4 mod 16: conflict-free DMMA fragments)
   double *Wq;       // QR work matrix (arena or global)
   int ldq;
   double *tile;     // GEMM/panel staging (arena tail)
@@ -174,10 +174,11 @@ __device__ __forceinline__ void blk_sum_n(double *v, double *red) {
 
 __device__ __forceinline__ long long ph_now() { return clock64(); }
 
-// Leading dimension of the delayed-update factors X, Yt: = 8 (mod 16), so the
-// 8 rows x 4 columns of a DMMA A/B fragment fall on distinct shared-memory
-// bank pairs (two wavefronts per fragment load).
-__host__ __device__ __forceinline__ int z2_ldx(int N) { return ((N + 15) & ~15) + 8; }
+// Leading dimension of the delayed-update factors X, Yt: = 4 (mod 16), so
+// each half-warp's 4 rows x 4 columns of a DMMA A/B fragment (row + 4 column
+// mod 16) fall on distinct shared-memory bank pairs (two wavefronts per
+// fragment load).
+__host__ __device__ __forceinline__ int z2_ldx(int N) { return ((N + 15) & ~15) + 4; }
 
 // ranf multiplier powers IP^i mod 2^31, i = 0..32 (filled by the host).
 __constant__ unsigned int c_ipow[33];
