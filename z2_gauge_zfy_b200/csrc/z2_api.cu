@@ -190,6 +190,33 @@ struct HostLattice {
   }
 };
 
+// L when the checkerboard table of an L x L lattice has the layout the fused
+// kinetic kernels assume (group 0/1: x bonds from odd/even x, slot
+// y L/2 + m; group 2/3: y bonds from odd/even y, slot m L + x; bond
+// orientation (site, next site)), else 0.
+int kin_fused_size(const HostLattice &lat) {
+  const int L = lat.Lx;
+  if (lat.Ly != L || L % 2 != 0 || L < 4 || L > 16 || !lat.ok) return 0;
+  const int H = L * L / 2, HL = L / 2;
+  auto check = [&](int g, int slot, int a, int b) {
+    const int bd = lat.groups[g * H + slot];
+    return lat.bonds[2 * bd] == a && lat.bonds[2 * bd + 1] == b;
+  };
+  for (int y = 0; y < L; ++y)
+    for (int m = 0; m < HL; ++m) {
+      const int xo = 2 * m + 1, xe = 2 * m;
+      if (!check(0, y * HL + m, y * L + xo, y * L + (xo + 1) % L)) return 0;
+      if (!check(1, y * HL + m, y * L + xe, y * L + xe + 1)) return 0;
+    }
+  for (int m = 0; m < HL; ++m)
+    for (int x = 0; x < L; ++x) {
+      const int yo = 2 * m + 1, ye = 2 * m;
+      if (!check(2, m * L + x, yo * L + x, ((yo + 1) % L) * L + x)) return 0;
+      if (!check(3, m * L + x, ye * L + x, (ye + 1) * L + x)) return 0;
+    }
+  return L;
+}
+
 struct ChainHost {
   z2_chain_params p;
   int N, Ltrot, Nst, nb;
@@ -533,6 +560,7 @@ extern "C" int z2_create(z2_handle **out, const z2_chain_params *params, int32_t
       d.ptime = std::max(0.0, std::min(1.0, pt));
     }
     d.hzero = std::fabs(p.h) <= kZero ? 1 : 0;
+    d.kin_fused = kin_fused_size(lat);
     d.bonds = (const int *)(base + o_bonds); d.groups = (const int *)(base + o_groups);
     d.bbonds = (const int *)(base + o_bb); d.plaq = (const int *)(base + o_plaq);
     d.xy = (const int *)(base + o_xy); d.nbx = (const int *)(base + o_nbx);

@@ -69,6 +69,16 @@ __device__ __noinline__ void build_table(const ChainDesc &c, const Smem &s, int 
   __syncthreads();
 }
 
+// One bond of a checkerboard group (process_group): [a, b] <- [[C, S], [S, C]]
+// [a, b], with the rounding sequence fixed (one product, one FMA per output)
+// so that every kinetic kernel below gives the same bits.
+__device__ __forceinline__ void kin_rot(double &a, double &b, double C, double S) {
+  const double na = __fma_rn(C, a, __dmul_rn(S, b));
+  const double nb = __fma_rn(S, a, __dmul_rn(C, b));
+  a = na;
+  b = nb;
+}
+
 // M <- B^nflag M : rows P1, P2 rotated by [[C,S],[S,C]] (process_group).
 // Row rotations never mix columns, so one thread carries its column through
 // all eight group passes: no barrier between passes.
@@ -96,21 +106,129 @@ __device__ __forceinline__ void kin_group_vec(const Smem &s, double *base, size_
     for (int q = 0; q < 8; ++q) { a[q] = base[pp[q].x * stride]; b[q] = base[pp[q].y * stride]; }
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-      base[pp[q].x * stride] = C[q] * a[q] + S[q] * b[q];
-      base[pp[q].y * stride] = S[q] * a[q] + C[q] * b[q];
+      kin_rot(a[q], b[q], C[q], S[q]);
+      base[pp[q].x * stride] = a[q];
+      base[pp[q].y * stride] = b[q];
     }
   }
   for (; kq < half; ++kq) {
     const int2 pp = tp2[g0 + kq];
     const double C = tc[g0 + kq], S = fl * ts[g0 + kq];
-    const double a = base[pp.x * stride], b = base[pp.y * stride];
-    base[pp.x * stride] = C * a + S * b;
-    base[pp.y * stride] = S * a + C * b;
+    double a = base[pp.x * stride], b = base[pp.y * stride];
+    kin_rot(a, b, C, S);
+    base[pp.x * stride] = a;
+    base[pp.y * stride] = b;
+  }
+}
+
+// Fused passes on an L x L lattice with periodic boundaries (sites
+// y L + x).  The four groups are the x bonds from odd x (group 0) and from
+// even x (group 1), and the y bonds from odd y (group 2) and from even y
+// (group 3), each listed row by row (HostLattice, src/lattice.f90:72-102):
+//   group 0: bond (y L + x, y L + x+1 mod L), x = 2m+1, table slot y L/2 + m
+//   group 1: x = 2m, same slots;  group 2: (y L + x, (y+1 mod L) L + x),
+//   y = 2m+1, slot m L + x;  group 3: y = 2m, same slots.
+// Groups 0 and 1 only mix the sites of one lattice row and groups 2 and 3
+// only those of one lattice column, so the pass sequence 0 1 | 2 3 3 2 | 1 0
+// runs as three sweeps over lines: a thread loads one line of one matrix
+// column (or row) into registers, applies its passes and stores it, instead
+// of streaming the whole matrix through shared memory once per pass.  The
+// rotations and their order within each bond are those of the pass-by-pass
+// kernel, so the results are bitwise equal.
+template <int L>
+__device__ __forceinline__ void kin_line_odd(double (&v)[L], const double *__restrict__ tc,
+                                             const double *__restrict__ ts, double fl, int q0,
+                                             int qs) {
+#pragma unroll
+  for (int m = 0; m < L / 2; ++m) {
+    const int q = q0 + m * qs;
+    kin_rot(v[2 * m + 1], v[(2 * m + 2) % L], tc[q], fl * ts[q]);
+  }
+}
+template <int L>
+__device__ __forceinline__ void kin_line_even(double (&v)[L], const double *__restrict__ tc,
+                                              const double *__restrict__ ts, double fl, int q0,
+                                              int qs) {
+#pragma unroll
+  for (int m = 0; m < L / 2; ++m) {
+    const int q = q0 + m * qs;
+    kin_rot(v[2 * m], v[2 * m + 1], tc[q], fl * ts[q]);
+  }
+}
+
+// The three sweeps for n independent vectors: vector i's site k sits at
+// M[i * vs + k * ks] (kin_rows: vs = ld, ks = 1; kin_cols: vs = 1, ks = ld).
+// Threads take (vector, line) pairs, vector fastest, so a warp touches one
+// line of 32 consecutive vectors.
+template <int L>
+__device__ __noinline__ void kin_fused(const Smem &s, double *M, size_t vs, size_t ks, int n,
+                                       int nflag) {
+  constexpr int H = L * L / 2, HL = L / 2;
+  const double fl = (double)nflag;
+  const double *__restrict__ tc = s.tc;
+  const double *__restrict__ ts = s.ts;
+  const int tasks = n * L;
+  // groups 0, 1 on lattice rows
+  for (int t = threadIdx.x; t < tasks; t += Z2_NT) {
+    const int i = t % n, y = t / n;
+    double *p = M + (size_t)i * vs + (size_t)(y * L) * ks;
+    double v[L];
+#pragma unroll
+    for (int x = 0; x < L; ++x) v[x] = p[(size_t)x * ks];
+    kin_line_odd<L>(v, tc, ts, fl, y * HL, 1);
+    kin_line_even<L>(v, tc, ts, fl, H + y * HL, 1);
+#pragma unroll
+    for (int x = 0; x < L; ++x) p[(size_t)x * ks] = v[x];
+  }
+  __syncthreads();
+  // groups 2, 3, 3, 2 on lattice columns
+  for (int t = threadIdx.x; t < tasks; t += Z2_NT) {
+    const int i = t % n, x = t / n;
+    double *p = M + (size_t)i * vs + (size_t)x * ks;
+    double v[L];
+#pragma unroll
+    for (int y = 0; y < L; ++y) v[y] = p[(size_t)(y * L) * ks];
+    kin_line_odd<L>(v, tc, ts, fl, 2 * H + x, L);
+    kin_line_even<L>(v, tc, ts, fl, 3 * H + x, L);
+    kin_line_even<L>(v, tc, ts, fl, 3 * H + x, L);
+    kin_line_odd<L>(v, tc, ts, fl, 2 * H + x, L);
+#pragma unroll
+    for (int y = 0; y < L; ++y) p[(size_t)(y * L) * ks] = v[y];
+  }
+  __syncthreads();
+  // groups 1, 0 on lattice rows
+  for (int t = threadIdx.x; t < tasks; t += Z2_NT) {
+    const int i = t % n, y = t / n;
+    double *p = M + (size_t)i * vs + (size_t)(y * L) * ks;
+    double v[L];
+#pragma unroll
+    for (int x = 0; x < L; ++x) v[x] = p[(size_t)x * ks];
+    kin_line_even<L>(v, tc, ts, fl, H + y * HL, 1);
+    kin_line_odd<L>(v, tc, ts, fl, y * HL, 1);
+#pragma unroll
+    for (int x = 0; x < L; ++x) p[(size_t)x * ks] = v[x];
+  }
+  __syncthreads();
+}
+
+// kin_fused for the lattice sizes it is instantiated for; false otherwise.
+__device__ __forceinline__ bool kin_fused_any(int L, const Smem &s, double *M, size_t vs, size_t ks,
+                                              int n, int nflag) {
+  switch (L) {
+    case 4: kin_fused<4>(s, M, vs, ks, n, nflag); return true;
+    case 6: kin_fused<6>(s, M, vs, ks, n, nflag); return true;
+    case 8: kin_fused<8>(s, M, vs, ks, n, nflag); return true;
+    case 10: kin_fused<10>(s, M, vs, ks, n, nflag); return true;
+    case 12: kin_fused<12>(s, M, vs, ks, n, nflag); return true;
+    case 14: kin_fused<14>(s, M, vs, ks, n, nflag); return true;
+    case 16: kin_fused<16>(s, M, vs, ks, n, nflag); return true;
+    default: return false;
   }
 }
 
 __device__ __noinline__ void kin_rows(const ChainDesc &c, const Smem &s, double *M, int ld, int ncols,
                          int nflag) {
+  if (kin_fused_any(c.kin_fused, s, M, (size_t)ld, 1, ncols, nflag)) return;
   const int half = c.half;
   const double fl = (double)nflag;
   for (int col = threadIdx.x; col < ncols; col += Z2_NT) {
@@ -124,6 +242,7 @@ __device__ __noinline__ void kin_rows(const ChainDesc &c, const Smem &s, double 
 // row through all eight passes.
 __device__ __noinline__ void kin_cols(const ChainDesc &c, const Smem &s, double *M, int ld, int nrows,
                          int nflag) {
+  if (kin_fused_any(c.kin_fused, s, M, 1, (size_t)ld, nrows, nflag)) return;
   const int half = c.half;
   const double fl = (double)nflag;
   for (int row = threadIdx.x; row < nrows; row += Z2_NT) {

@@ -55,6 +55,8 @@ struct ChainDesc {
   double rb[9];     // boson ratio table [(ds+4)/4 * 3 + (dt+4)/4]
   int use_kin;      // RT > Zero (src/local_sweep.f90:96, dynamics.f90:57)
   int hzero;        // |h| <= Zero (src/local_sweep.f90:64)
+  int kin_fused;    // L when the bond table has the square-lattice layout of
+                    // kin_rows_fused / kin_cols_fused (host-checked), else 0
   // lattice tables (device)
   const int *bonds;     // [2N][2] endpoints (0-based sites)
   const int *groups;    // [4][half] bond ids of checkerboard groups 1..4
