@@ -521,7 +521,7 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
     for (int q = 0; q < 6; ++q) bbs[6 * i + q] = (short)c.bbonds[6 * i + q];
   }
   __syncthreads();
-  double *pdat = s.red + 48;      // accepted proposal: pinv(4), D11, D12
+  double *pdat = s.red + 48;      // accepted proposal: Prod(4), D11, D12, det(Prod)
   const int *__restrict__ bond = s.bond;
   volatile int *flag = s.flag;
   unsigned int st = 0;
@@ -571,9 +571,6 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
       const double m22 = __dadd_rn(__dmul_rn(D12, l12), __dmul_rn(D11, l22));
       const double p11 = __dadd_rn(1.0, m11), p12 = m12, p21 = m21, p22 = __dadd_rn(1.0, m22);
       const double det = __dsub_rn(__dmul_rn(p11, p22), __dmul_rn(p12, p21));
-      // Prod^-1 entries in every lane, ahead of the ballot (off the path of
-      // the accepting lane)
-      const double idet = 1.0 / det;
       // boson ratio (src/fields.f90:40-119) from the host table
       const short *bb = bbs + 6 * b;
       const double tmp_old = s_old * sig[bb[0]] * sig[bb[1]] * sig[bb[2]] +
@@ -597,8 +594,10 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
         if (c.ratios) c.ratios[li] = ratio;
       }
       if (lane == first) {
-        pdat[0] = p22 * idet; pdat[1] = -p12 * idet; pdat[2] = -p21 * idet; pdat[3] = p11 * idet;
-        pdat[4] = D11; pdat[5] = D12;
+        // Prod and its determinant; the inverse is formed by the column
+        // phase, where the division overlaps the loads of G, X and Yt
+        pdat[0] = p11; pdat[1] = p12; pdat[2] = p21; pdat[3] = p22;
+        pdat[4] = D11; pdat[5] = D12; pdat[6] = det;
         flag[1] = b;
       }
       st = ranf_adv(st, cnt);
@@ -618,7 +617,9 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
     const int b = flag[1];
     if (b >= 0) {
       const int p1 = bond[2 * b], p2 = bond[2 * b + 1];
-      const double q00 = pdat[0], q01 = pdat[1], q10 = pdat[2], q11 = pdat[3];
+      const double idet = 1.0 / pdat[6];
+      const double q00 = pdat[3] * idet, q01 = -pdat[1] * idet, q10 = -pdat[2] * idet,
+                   q11 = pdat[0] * idet;
       const double D11 = pdat[4], D12 = pdat[5];
       for (int i = threadIdx.x; i < N; i += Z2_NT) {
         double u0 = G[i + (size_t)p1 * ldg], u1 = G[i + (size_t)p2 * ldg];

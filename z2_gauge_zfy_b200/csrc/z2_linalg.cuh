@@ -215,11 +215,17 @@ __device__ __noinline__ void blk_geqr2(double *A, int lda, int m, int n, double 
 
 // QDRP_decompose's split (src/stabilization.f90:61-66): D(i) = |R(i,i)|,
 // R(i, i:n) /= D(i).
-__device__ __noinline__ void blk_qdrp_scale(double *A, int lda, int n, double *D) {
-  for (int i = threadIdx.x; i < n; i += Z2_NT) D[i] = fabs(A[i + (size_t)i * lda]);
+// The rows are scaled by the reciprocal of D (one division per row instead
+// of one per element; rd: n doubles of scratch, left holding 1/D).
+__device__ __noinline__ void blk_qdrp_scale(double *A, int lda, int n, double *D, double *rd) {
+  for (int i = threadIdx.x; i < n; i += Z2_NT) {
+    const double d = fabs(A[i + (size_t)i * lda]);
+    D[i] = d;
+    rd[i] = 1.0 / d;
+  }
   __syncthreads();
   for (int j = threadIdx.x / 32; j < n; j += Z2_WARPS)
-    for (int i = threadIdx.x & 31; i <= j; i += 32) A[i + (size_t)j * lda] = A[i + (size_t)j * lda] / D[i];
+    for (int i = threadIdx.x & 31; i <= j; i += 32) A[i + (size_t)j * lda] = A[i + (size_t)j * lda] * rd[i];
   __syncthreads();
 }
 

@@ -13,7 +13,7 @@ __device__ __noinline__ void dev_stab_U(const Smem &s, int N, double *A, int lda
   int *jpvt = s.ivec;
   blk_scale_cols(A, lda, N, N, D);                 // matUDV(:,i) *= D(i)
   blk_geqp3_fast(A, lda, N, jpvt, tau, vn1, vn2, s.tile, s.tile_doubles, s.red);   // ZGEQP3
-  blk_qdrp_scale(A, lda, N, Dn);                   // D = |R_ii|, R rows /= D
+  blk_qdrp_scale(A, lda, N, Dn, vn2);              // D = |R_ii|, R rows /= D
   for (int i = threadIdx.x; i < N; i += Z2_NT) D[i] = Dn[i];
   if (!left) {
     // VR <- R (P^T VR)     (ZLAPMR(.true.) + ZTRMM('L','U','N','N'))
@@ -68,7 +68,7 @@ __device__ __noinline__ void dev_stab_green(const Smem &s, int N, int nt, int Lt
     __syncthreads();
   }
   blk_geqp3_fast(M, ldm, N, jpvt, tau, vn1, vn2, s.tile, s.tile_doubles, s.red);
-  blk_qdrp_scale(M, ldm, N, Dn);
+  blk_qdrp_scale(M, ldm, N, Dn, vn2);   // vn2 keeps 1/D for the D^-1 scalings below
   // keep the scaled R (upper triangle) for the triangular solve
   for (int j = threadIdx.x / 32; j < N; j += Z2_WARPS)
     for (int i = threadIdx.x & 31; i <= j; i += 32) W3[i + (size_t)j * N] = M[i + (size_t)j * ldm];
@@ -80,7 +80,7 @@ __device__ __noinline__ void dev_stab_green(const Smem &s, int N, int nt, int Lt
     // Y = D^-1 (Q^T UR^T) back into the arena (Q is no longer needed)
     for (int j = threadIdx.x / 32; j < N; j += Z2_WARPS)
       for (int i = threadIdx.x & 31; i < N; i += 32)
-        M[i + (size_t)j * ldm] = W2[i + (size_t)j * N] / Dn[i];
+        M[i + (size_t)j * ldm] = W2[i + (size_t)j * N] * vn2[i];
     __syncthreads();
     blk_trsm_lun_blocked(W3, N, N, M, ldm, N);     // R_s^-1 Y
     blk_perm_rows(W1, N, M, ldm, N, N, jpvt, false);   // ZLAPMR(.false.)
@@ -90,7 +90,7 @@ __device__ __noinline__ void dev_stab_green(const Smem &s, int N, int nt, int Lt
     blk_dmma(N, N, N, 1.0, MatRef{ULT, 1, N}, false, MatRef{M, 1, ldm}, false, 0.0, W2, N);
     for (int j = threadIdx.x / 32; j < N; j += Z2_WARPS)
       for (int i = threadIdx.x & 31; i < N; i += 32)
-        M[i + (size_t)j * ldm] = W2[j + (size_t)i * N] / Dn[i];
+        M[i + (size_t)j * ldm] = W2[j + (size_t)i * N] * vn2[i];
     __syncthreads();
     blk_trsm_lun_blocked(W3, N, N, M, ldm, N);     // X^T
     blk_perm_rows(W1, N, M, ldm, N, N, jpvt, false);   // (X P^T)^T
