@@ -297,9 +297,52 @@ __device__ __noinline__ void blk_orgqr(double *A, int lda, int n, const double *
     __syncthreads();
     // S = V^T V
     blk_dmma(ib, ib, mp, 1.0, MatRef{V, ldv, 1}, false, MatRef{V, 1, ldv}, false, 0.0, S, ib);
-    // T (DLARFT): T(c,c) = tau_c, T(r,c) = -tau_c sum_{r<=q<c} T(r,q) S(q,c).
-    // Row r depends only on itself, so thread r builds it in registers.
-    if (tid < ib) {
+    // T (DLARFT).  T is the inverse of the upper-triangular matrix with
+    // diagonal 1/tau and strict upper part S (DLARFT's column recurrence is
+    // exactly the forward substitution of that inverse); warp 0 forms it by
+    // doubling: diagonal blocks of size b pair up as T12 = -T11 S12 T22, four
+    // levels of short dot products instead of 16 dependent columns.  A zero
+    // tau zeroes its row and column, as in DLARFT.  Needs 4 nb doubles of
+    // scratch in W; without them the per-row recurrence runs.
+    if (ldw * (n - nb) >= 4 * nb) {
+      double *Xs = W;
+      if (tid < 32) {
+        for (int e = tid; e < ib * ib; e += 32) {
+          const int r = e % ib, c = e / ib;
+          T[e] = (r == c) ? tau[i0 + c] : 0.0;
+        }
+        __syncwarp();
+        for (int b = 1; b < ib; b <<= 1) {
+          const int np = (ib + 2 * b - 1) / (2 * b), bb = b * b;
+          for (int e = tid; e < np * bb; e += 32) {
+            const int p = e / bb, r = (e % bb) % b, c = (e % bb) / b;
+            const int k = 2 * b * p, k2 = k + b;
+            if (k2 + c < ib) {
+              double x0 = 0.0, x1 = 0.0;
+              for (int q = 0; q <= c; q += 2) {
+                x0 += S[(k + r) + (k2 + q) * ib] * T[(k2 + q) + (k2 + c) * ib];
+                if (q + 1 <= c) x1 += S[(k + r) + (k2 + q + 1) * ib] * T[(k2 + q + 1) + (k2 + c) * ib];
+              }
+              Xs[e] = x0 + x1;
+            }
+          }
+          __syncwarp();
+          for (int e = tid; e < np * bb; e += 32) {
+            const int p = e / bb, r = (e % bb) % b, c = (e % bb) / b;
+            const int k = 2 * b * p, k2 = k + b;
+            if (k2 + c < ib) {
+              double t0 = 0.0, t1 = 0.0;
+              for (int q = r; q < b; q += 2) {
+                t0 += T[(k + r) + (k + q) * ib] * Xs[p * bb + q + c * b];
+                if (q + 1 < b) t1 += T[(k + r) + (k + q + 1) * ib] * Xs[p * bb + q + 1 + c * b];
+              }
+              T[(k + r) + (k2 + c) * ib] = -(t0 + t1);
+            }
+          }
+          __syncwarp();
+        }
+      }
+    } else if (tid < ib) {
       const int r = tid;
       double tr[16];
 #pragma unroll
