@@ -44,14 +44,16 @@ def test_seeded_config_bit_exact():
         assert iseed == rng.state, absolute
 
 
-@pytest.mark.parametrize("L", [4, 6, 8])
-def test_mmult_parity(L):
-    ch = Chain(RT=1.0, Nlx=L, Nly=L, Ltrot=20, beta=2.0, Nwrap=10, seed=777)
+@pytest.mark.parametrize("Lx,Ly", [(4, 4), (6, 6), (8, 8), (12, 12), (4, 6), (6, 4)])
+def test_mmult_parity(Lx, Ly):
+    """B^nflag M and M B^nflag (mmult_R / mmult_L).  Square lattices take the
+    fused line kernels, rectangular ones the pass-by-pass kernel."""
+    ch = Chain(RT=1.0, Nlx=Lx, Nly=Ly, Ltrot=20, beta=2.0, Nwrap=10, seed=777)
     rng = np.random.default_rng(1)
-    N = L * L
+    N = Lx * Ly
     with Z2Batch([ch]) as b:
         p = oracle_params(ch)
-        lat = zo.Lattice(L, L)
+        lat = zo.Lattice(Lx, Ly)
         sig, _, _ = zo.seeded_config(p, lat, ch.seed)
         opk = zo.OperatorKin(p, lat)
         for nt in (1, 7, 20):
@@ -198,6 +200,22 @@ def test_sweep_parity_c1():
     for k, v in c.obs.as_dict().items():
         assert abs(obs[k] - v) <= RTOL * max(abs(v), 1.0), k
     assert abs(st["Xmaxm"] - c.prop.Xmaxm) <= 1e-9 * max(c.prop.Xmaxm, 1e-3)
+
+
+@pytest.mark.parametrize("Lx,Ly", [(4, 6), (6, 4)])
+def test_sweep_parity_rectangular(Lx, Ly):
+    """Lx != Ly: the pass-by-pass checkerboard kernel (the fused line kernels
+    only take square lattices); decisions bit-exact, G within tolerance."""
+    ch = Chain(RT=1.0, J=0.5, h=0.5, mu=0.0, Nlx=Lx, Nly=Ly, Ltrot=20, beta=2.0, Nwrap=5,
+               seed=2024)
+    c, res = _run_pair(ch, nbins=1)
+    G, obs, st, (dec, rat), _, (sig, iseed), _ = res[-1]
+    dec_o, rat_o = _decisions_oracle(c, ch.Ltrot, 2 * ch.N)
+    assert np.array_equal(dec, dec_o)
+    assert np.array_equal(sig, c.sigma)
+    assert rel(G, c.prop.Gr) < RTOL
+    for k, v in c.obs.as_dict().items():
+        assert abs(obs[k] - v) <= RTOL * max(abs(v), 1.0), k
 
 
 def test_sweep_parity_mu_replay_all_accept():
