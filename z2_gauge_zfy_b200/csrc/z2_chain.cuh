@@ -698,23 +698,36 @@ __device__ __noinline__ void obs_equal(const ChainDesc &c, const Smem &s, int nt
     v[4] += n + n;
   }
   const int W = 2 * c.Lx - 1;
-  for (int e = threadIdx.x; e < N * N; e += Z2_NT) {
-    const int i = e % N, j = e / N;
-    const double gij = G[i + (size_t)j * ldg], gji = G[j + (size_t)i * ldg];
-    const double ni = 1.0 - G[i + (size_t)i * ldg], nj = 1.0 - G[j + (size_t)j * ldg];
-    const double dl = (i == j) ? 1.0 : 0.0;
-    const double pq = dl - gij;
-    v[1] += pq * pq;
-    const double a = ni * nj;
-    const double ex = (dl - gji) * gij;
-    double dc = a - ex;
-    dc = (dc + a) - ex;
-    dc = (dc + a) + a;
-    const double ph = c.stag[i] * c.stag[j];
-    const int dx = c.xy[2 * i] - c.xy[2 * j], dy = c.xy[2 * i + 1] - c.xy[2 * j + 1];
-    const double ps = c.pshift[(dx + c.Lx - 1) + (dy + c.Ly - 1) * W];
-    v[2] += ph * dc;
-    v[3] += ps * dc;
+  // task = (row i, one third of the columns j): the row's density, phase
+  // and coordinates stay in registers, the warp's lanes take consecutive
+  // rows (G(i, j) contiguous, G(j, i) at the odd stride, column values
+  // broadcast), and no element needs an index division
+  const int J3 = (N + 2) / 3;
+  for (int t = threadIdx.x; t < 3 * N; t += Z2_NT) {
+    const int i = t % N, j0 = (t / N) * J3;
+    const int j1 = (j0 + J3 < N) ? j0 + J3 : N;
+    const double ni = 1.0 - G[i + (size_t)i * ldg];
+    const double sti = c.stag[i];
+    const int xi = c.xy[2 * i] + c.Lx - 1, yi = c.xy[2 * i + 1] + c.Ly - 1;
+    const double *gi = G + i, *gj = G + (size_t)i * ldg;
+#pragma unroll 4
+    for (int j = j0; j < j1; ++j) {
+      const double gij = gi[(size_t)j * ldg], gji = gj[j];
+      const double nj = 1.0 - G[j + (size_t)j * ldg];
+      const double dl = (i == j) ? 1.0 : 0.0;
+      const double pq = dl - gij;
+      v[1] += pq * pq;
+      const double a = ni * nj;
+      const double ex = (dl - gji) * gij;
+      double dc = a - ex;
+      dc = (dc + a) - ex;
+      dc = (dc + a) + a;
+      const double ph = sti * c.stag[j];
+      const int dx = xi - c.xy[2 * j], dy = yi - c.xy[2 * j + 1];
+      const double ps = c.pshift[dx + dy * W];
+      v[2] += ph * dc;
+      v[3] += ps * dc;
+    }
   }
   blk_sum_n<5>(v, s.red);
   if (threadIdx.x == 0) {
