@@ -290,10 +290,9 @@ __device__ __noinline__ void blk_orgqr(double *A, int lda, int n, const double *
     const int ib = (n - i0) < nb ? (n - i0) : nb;
     const int mp = n - i0, nc = n - i0 - ib;
     // V: unit lower trapezoidal, mp x ib
-    for (int e = tid; e < mp * ib; e += Z2_NT) {
-      const int r = e % mp, c = e / mp;
-      V[r + (size_t)c * ldv] = (r == c) ? 1.0 : (r > c ? A[(i0 + r) + (size_t)(i0 + c) * lda] : 0.0);
-    }
+    for (int c = tid >> 5; c < ib; c += Z2_WARPS)
+      for (int r = tid & 31; r < mp; r += 32)
+        V[r + (size_t)c * ldv] = (r == c) ? 1.0 : (r > c ? A[(i0 + r) + (size_t)(i0 + c) * lda] : 0.0);
     __syncthreads();
     // S = V^T V
     blk_dmma(ib, ib, mp, 1.0, MatRef{V, ldv, 1}, false, MatRef{V, 1, ldv}, false, 0.0, S, ib);
@@ -401,10 +400,8 @@ __device__ __noinline__ void blk_orgqr(double *A, int lda, int n, const double *
       for (int q = r; q <= c; ++q) t += T[r + q * ib] * V[c + (size_t)q * ldv];
       S[r + c * ib] = t;
     }
-    for (int e = tid; e < n * ib; e += Z2_NT) {
-      const int r = e % n, c = e / n;
-      A[r + (size_t)(i0 + c) * lda] = (r == i0 + c) ? 1.0 : 0.0;
-    }
+    for (int c = tid >> 5; c < ib; c += Z2_WARPS)
+      for (int r = tid & 31; r < n; r += 32) A[r + (size_t)(i0 + c) * lda] = (r == i0 + c) ? 1.0 : 0.0;
     __syncthreads();
     blk_dmma(mp, ib, ib, -1.0, MatRef{V, 1, ldv}, false, MatRef{S, 1, ib}, false, 1.0,
              A + i0 + (size_t)i0 * lda, lda);
@@ -476,10 +473,9 @@ __device__ __noinline__ void blk_geqrf(double *A, int lda, int n, double *tau, d
     }
     if (nc <= 0) continue;
     // ---- V (unit lower), S = V^T V, T (DLARFT) ----
-    for (int e = tid; e < mp * ib; e += Z2_NT) {
-      const int r = e % mp, c = e / mp;
-      V[r + (size_t)c * ldv] = (r == c) ? 1.0 : (r > c ? A[(j0 + r) + (size_t)(j0 + c) * lda] : 0.0);
-    }
+    for (int c = tid >> 5; c < ib; c += Z2_WARPS)
+      for (int r = tid & 31; r < mp; r += 32)
+        V[r + (size_t)c * ldv] = (r == c) ? 1.0 : (r > c ? A[(j0 + r) + (size_t)(j0 + c) * lda] : 0.0);
     __syncthreads();
     blk_dmma(ib, ib, mp, 1.0, MatRef{V, ldv, 1}, false, MatRef{V, 1, ldv}, false, 0.0, S, ib);
     if (tid < ib) {
@@ -687,6 +683,11 @@ __device__ __noinline__ void blk_trsm_lun_blocked(const double *R, int ldr, int 
 #pragma unroll
       for (int q = 0; q < 8; ++q)
         rr[p][q] = (p <= q && q < kb) ? R[(k0 + p) + (size_t)(k0 + q) * ldr] : 0.0;
+    // reciprocals of the diagonal: one division per entry instead of one per
+    // entry and right-hand side, off the columns' dependent chains
+    double rd[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) rd[q] = (q < kb) ? 1.0 / rr[q][q] : 0.0;
     for (int j = threadIdx.x; j < nc; j += Z2_NT) {
       double *Yj = Y + (size_t)j * ldy + k0;
       double y[8];
@@ -697,7 +698,7 @@ __device__ __noinline__ void blk_trsm_lun_blocked(const double *R, int ldr, int 
         if (q < kb) {
           double z = y[q];
           if (z != 0.0) {
-            z = z / rr[q][q];
+            z = z * rd[q];
             y[q] = z;
 #pragma unroll
             for (int p = 0; p < 8; ++p)

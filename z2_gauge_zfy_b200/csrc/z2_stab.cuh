@@ -57,14 +57,12 @@ __device__ __noinline__ void dev_stab_green(const Smem &s, int N, int nt, int Lt
   __syncthreads();
   const int half = Ltrot / 2;
   if (nt > half) {   // matUDV = matUDV^dagger
-    for (int e = threadIdx.x; e < N * N; e += Z2_NT) {
-      const int i = e % N, j = e / N;
-      if (i < j) {
+    for (int j = threadIdx.x / 32; j < N; j += Z2_WARPS)
+      for (int i = threadIdx.x & 31; i < j; i += 32) {
         const double a = M[i + (size_t)j * ldm], b = M[j + (size_t)i * ldm];
         M[i + (size_t)j * ldm] = b;
         M[j + (size_t)i * ldm] = a;
       }
-    }
     __syncthreads();
   }
   blk_geqp3_fast(M, ldm, N, jpvt, tau, vn1, vn2, s.tile, s.tile_doubles, s.red);
