@@ -17,7 +17,8 @@
 // Pivoting follows DGEQP3 without moving data: the logical position of every
 // physical column is tracked (pos / lp2c), the arg-max breaks ties by logical
 // position as IDAMAX does on the swapped arrays, and the partial norm
-// downdate and its recompute threshold are DLAQP2's.  Each column is written
+// downdate and its recompute threshold are DLAQP2's (its test and update
+// multiplied out by vn1^2, so that no division sits on the step).  Each column is written
 // to A at the step that factors it, at its logical position, so the result
 // has DGEQP3's layout (R above the diagonal, reflectors below, tau, 1-based
 // jpvt).
@@ -64,6 +65,71 @@ __device__ __forceinline__ int block_pivot(const double *wmax, const int *wpos, 
   warp_argmax_vp(v, p, bv, bp);
   const unsigned w = __ballot_sync(Z2_FULL, lane < Z2_WARPS && p == bp);
   return __shfl_sync(Z2_FULL, c, w ? __ffs(w) - 1 : 0);
+}
+
+// Column sums of the trailing dot products over the 16 lanes of a column
+// group, in every lane.  For S >= 5 the first 8 column slots are reduced by
+// halving (lanes that differ in bit 8 / 4 / 2 of tr swap halves of what they
+// hold, then the last bit is a plain exchange), which leaves each column's
+// sum in two lanes after 4 + 2 + 1 + 1 exchanges, and the sums are then
+// broadcast (8 more); slot 8 takes the plain butterfly.  Each sum is formed
+// by the same pairwise additions as the four-level butterfly over all slots
+// (36 exchanges), so the result is the same to the bit.
+template <int S>
+__device__ __forceinline__ void qrp_colsum8(double (&d)[S], int tr, int hl);
+template <int S>
+__device__ __forceinline__ void qrp_colsum(double (&d)[S], int tr, int hl) {
+  if (S < 5) {
+#pragma unroll
+    for (int o = 8; o; o >>= 1) {
+#pragma unroll
+      for (int q = 0; q < S; ++q) d[q] += __shfl_xor_sync(Z2_FULL, d[q], o);
+    }
+  } else {
+    qrp_colsum8<S>(d, tr, hl);
+  }
+}
+
+template <int S>
+__device__ __forceinline__ void qrp_colsum8(double (&d)[S], int tr, int hl) {
+  double e[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) e[q] = (q < S) ? d[q < S ? q : 0] : 0.0;
+  // bit 8: keep slots [0,4) (bit clear) or [4,8) (bit set)
+  const bool b8 = tr & 8, b4 = tr & 4, b2 = tr & 2;
+  double f[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const double send = b8 ? e[k] : e[4 + k];
+    const double keep = b8 ? e[4 + k] : e[k];
+    f[k] = keep + __shfl_xor_sync(Z2_FULL, send, 8);
+  }
+  double g[2];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const double send = b4 ? f[k] : f[2 + k];
+    const double keep = b4 ? f[2 + k] : f[k];
+    g[k] = keep + __shfl_xor_sync(Z2_FULL, send, 4);
+  }
+  double h;
+  {
+    const double send = b2 ? g[0] : g[1];
+    const double keep = b2 ? g[1] : g[0];
+    h = keep + __shfl_xor_sync(Z2_FULL, send, 2);
+  }
+  h += __shfl_xor_sync(Z2_FULL, h, 1);
+  // lane tr now holds slot 4 (tr>>3 & 1) + 2 (tr>>2 & 1) + (tr>>1 & 1)
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const double x = __shfl_sync(Z2_FULL, h, hl | (((q >> 2) & 1) << 3) | (((q >> 1) & 1) << 2) | ((q & 1) << 1));
+    if (q < S) d[q < S ? q : 0] = x;
+  }
+  if (S > 8) {
+    double x = d[S > 8 ? 8 : 0];
+#pragma unroll
+    for (int o = 8; o; o >>= 1) x += __shfl_xor_sync(Z2_FULL, x, o);
+    d[S > 8 ? 8 : 0] = x;
+  }
 }
 
 // Static-index views of the register tile: a[.][q] / a[p][.] for a warp-
@@ -239,11 +305,7 @@ __device__ __noinline__ void qrp_reg(double *A, int lda, int n, int *jpvt, doubl
         QRP_CASE_DOT(5) QRP_CASE_DOT(6) QRP_CASE_DOT(7) QRP_CASE_DOT(8)
         default: break;
       }
-#pragma unroll
-      for (int o = 8; o; o >>= 1) {
-#pragma unroll
-        for (int q = 0; q < S; ++q) d[q] += __shfl_xor_sync(Z2_FULL, d[q], o);
-      }
+      qrp_colsum<S>(d, tr, hl);
 #pragma unroll
       for (int q = 0; q < S; ++q) d[q] = ((done >> q) & 1u) ? 0.0 : t * d[q];
       switch (pj) {
@@ -275,14 +337,15 @@ __device__ __noinline__ void qrp_reg(double *A, int lda, int n, int *jpvt, doubl
     if (act) {
       v1 = vn1[cq];
       if (v1 != 0.0) {
-        double temp = fabs(ajc) / v1;
-        const double qq = v1 / vn2[cq];
-        temp = 1.0 - temp * temp;
-        temp = fmax(temp, 0.0);
-        if (temp * qq * qq <= tol3z) {
+        // DLAQP2's test temp (vn1/vn2)^2 <= tol3z with temp = 1 - (|a|/vn1)^2
+        // and its update vn1 sqrt(temp), multiplied out: (vn1^2 - a^2) is
+        // formed as (vn1 - |a|)(vn1 + |a|), so no division sits on the step
+        const double aa = fabs(ajc), w2 = vn2[cq];
+        const double r2 = fmax((v1 - aa) * (v1 + aa), 0.0);
+        if (r2 <= tol3z * (w2 * w2)) {
           need = true;
         } else {
-          v1 = v1 * sqrt(temp);
+          v1 = sqrt(r2);
           vn1[cq] = v1;
         }
       }
