@@ -522,6 +522,12 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
   }
   __syncthreads();
   double *pdat = s.red + 48;      // accepted proposal: Prod(4), D11, D12, det(Prod)
+  // rows p1, p2 of Yt and X of the accepted bond, interleaved per column q
+  // ([q][Yt(p1), Yt(p2), X(p1), X(p2)]), staged by warp 0 after its ballot
+  // so that the column phase reads them as 16-byte pairs
+  const int soff = (7 * N + 1) & ~1;
+  double *stg = s.vec + soff;
+  const bool staged = 4 * k2 <= 8 * N - soff;
   const int *__restrict__ bond = s.bond;
   volatile int *flag = s.flag;
   unsigned int st = 0;
@@ -600,6 +606,14 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
         pdat[4] = D11; pdat[5] = D12; pdat[6] = det;
         flag[1] = b;
       }
+      if (first < 32 && staged) {
+        const int f1 = __shfl_sync(Z2_FULL, p1, first), f2 = __shfl_sync(Z2_FULL, p2, first);
+        for (int q = lane; q < m; q += 32) {
+          const size_t oq = (size_t)q * ldx;
+          double *d = stg + 4 * q;
+          d[0] = Yt[f1 + oq]; d[1] = Yt[f2 + oq]; d[2] = X[f1 + oq]; d[3] = X[f2 + oq];
+        }
+      }
       st = ranf_adv(st, cnt);
       rpos += cnt;
       den += cnt;
@@ -628,15 +642,30 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
           // m is even: two independent FMA chains per output
           double w0 = 0.0, w1 = 0.0, z0 = 0.0, z1 = 0.0;
           const double *xi_ = X + i, *yi_ = Yt + i;
-          const double *xp1 = X + p1, *xp2 = X + p2, *yp1 = Yt + p1, *yp2 = Yt + p2;
+          if (staged) {
+            const double2 *sp = reinterpret_cast<const double2 *>(stg);
 #pragma unroll 2
-          for (int q = 0; q < m; q += 2) {
-            const size_t o0 = (size_t)q * ldx, o1 = o0 + ldx;
-            const double xa = xi_[o0], ya = yi_[o0], xb = xi_[o1], yb = yi_[o1];
-            const double a1 = yp1[o0], a2 = yp2[o0], b1 = xp1[o0], b2 = xp2[o0];
-            const double c1 = yp1[o1], c2 = yp2[o1], d1 = xp1[o1], d2 = xp2[o1];
-            u0 -= xa * a1; u1 -= xa * a2; v0 -= b1 * ya; v1 -= b2 * ya;
-            w0 += xb * c1; w1 += xb * c2; z0 += d1 * yb; z1 += d2 * yb;
+            for (int q = 0; q < m; q += 2) {
+              const size_t o0 = (size_t)q * ldx, o1 = o0 + ldx;
+              const double xa = xi_[o0], ya = yi_[o0], xb = xi_[o1], yb = yi_[o1];
+              const double2 ya0 = sp[2 * q], xa0 = sp[2 * q + 1];
+              const double2 ya1 = sp[2 * q + 2], xa1 = sp[2 * q + 3];
+              const double a1 = ya0.x, a2 = ya0.y, b1 = xa0.x, b2 = xa0.y;
+              const double c1 = ya1.x, c2 = ya1.y, d1 = xa1.x, d2 = xa1.y;
+              u0 -= xa * a1; u1 -= xa * a2; v0 -= b1 * ya; v1 -= b2 * ya;
+              w0 += xb * c1; w1 += xb * c2; z0 += d1 * yb; z1 += d2 * yb;
+            }
+          } else {
+            const double *xp1 = X + p1, *xp2 = X + p2, *yp1 = Yt + p1, *yp2 = Yt + p2;
+#pragma unroll 2
+            for (int q = 0; q < m; q += 2) {
+              const size_t o0 = (size_t)q * ldx, o1 = o0 + ldx;
+              const double xa = xi_[o0], ya = yi_[o0], xb = xi_[o1], yb = yi_[o1];
+              const double a1 = yp1[o0], a2 = yp2[o0], b1 = xp1[o0], b2 = xp2[o0];
+              const double c1 = yp1[o1], c2 = yp2[o1], d1 = xp1[o1], d2 = xp2[o1];
+              u0 -= xa * a1; u1 -= xa * a2; v0 -= b1 * ya; v1 -= b2 * ya;
+              w0 += xb * c1; w1 += xb * c2; z0 += d1 * yb; z1 += d2 * yb;
+            }
           }
           u0 -= w0; u1 -= w1; v0 -= z0; v1 -= z1;
         }
