@@ -416,6 +416,16 @@ __device__ __noinline__ void green_big_extract(int N, const double *B3, double *
 // ---------------------------------------------------------------------------
 // Delayed rank-2 updates (LocalK_metro, src/localK.f90:45-173)
 // ---------------------------------------------------------------------------
+// The delayed-update factors X and Yt (N x k2 each) keep their columns in
+// interleaved pairs: element (i, q) sits at (q / 2) 2 ldx + 2 i + q % 2, so
+// the two columns an accepted flip adds are one 16-byte word per row (one
+// load in the ratio evaluation and in the column phase, one store), and a
+// DMMA fragment (rows r + 0..7, columns l + 0..3) still hits 16 distinct
+// bank pairs per half-warp for ldx = 4 (mod 16).
+__device__ __forceinline__ size_t xy_at(int i, int q, int ldx) {
+  return (size_t)(q >> 1) * (2 * ldx) + 2 * i + (q & 1);
+}
+
 // G <- G - X Yt^T over the m queued columns (ld ldx) when 8 TR and 8 TC
 // divide N: each warp owns (8 TR) x (8 TC) blocks of G, reads their old
 // values before its DMMA chain (the load latency overlaps the products) and
@@ -443,15 +453,15 @@ __device__ __noinline__ void flush_tiles(double *G, int ldg, const double *X, co
           old[a][b][e] = cp[8 * a + (size_t)(8 * b + e) * ldg];
           acc[a][b][e] = 0.0;
         }
-    const double *pa = X + r0 + lr + (size_t)lc * ldx;
-    const double *pb = Yt + c0 + lr + (size_t)lc * ldx;
+    const double *pa = X + xy_at(r0 + lr, lc, ldx);
+    const double *pb = Yt + xy_at(c0 + lr, lc, ldx);
 #pragma unroll 2
     for (int l0 = 0; l0 < m4; l0 += 4) {
       double fa[TR], fb[TC];
 #pragma unroll
-      for (int u = 0; u < TR; ++u) fa[u] = pa[8 * u];
+      for (int u = 0; u < TR; ++u) fa[u] = pa[16 * u];
 #pragma unroll
-      for (int v = 0; v < TC; ++v) fb[v] = pb[8 * v];
+      for (int v = 0; v < TC; ++v) fb[v] = pb[16 * v];
       pa += s4; pb += s4;
 #pragma unroll
       for (int u = 0; u < TR; ++u)
@@ -463,9 +473,9 @@ __device__ __noinline__ void flush_tiles(double *G, int ldg, const double *X, co
       const bool ok = lc < m - m4;
       double fa[TR], fb[TC];
 #pragma unroll
-      for (int u = 0; u < TR; ++u) fa[u] = ok ? pa[8 * u] : 0.0;
+      for (int u = 0; u < TR; ++u) fa[u] = ok ? pa[16 * u] : 0.0;
 #pragma unroll
-      for (int v = 0; v < TC; ++v) fb[v] = ok ? pb[8 * v] : 0.0;
+      for (int v = 0; v < TC; ++v) fb[v] = ok ? pb[16 * v] : 0.0;
 #pragma unroll
       for (int u = 0; u < TR; ++u)
 #pragma unroll
@@ -481,12 +491,62 @@ __device__ __noinline__ void flush_tiles(double *G, int ldg, const double *X, co
   __syncthreads();
 }
 
-// G <- G - X Yt^T over the m queued columns (ld ldx): one DMMA rank-m update.
+// The same update for any N: 16 x 16 groups with bounds checks (the k loop
+// and epilogue of blk_dmma's general path).
+__device__ __noinline__ void flush_generic(double *G, int ldg, const double *X, const double *Yt,
+                                           int N, int ldx, int m) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int lr = lane >> 2, lc = lane & 3;
+  const int gm = (N + 15) >> 4;
+  for (int g = warp; g < gm * gm; g += Z2_WARPS) {
+    const int r0 = (g % gm) << 4, c0 = (g / gm) << 4;
+    const int ra0 = r0 + lr, ra1 = ra0 + 8, cb0 = c0 + lr, cb1 = cb0 + 8;
+    double acc[2][2][2];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+    for (int l0 = 0; l0 < m; l0 += 4) {
+      const int l = l0 + lc;
+      const bool lk = l < m;
+      const double a0 = (lk && ra0 < N) ? X[xy_at(ra0, l, ldx)] : 0.0;
+      const double a1 = (lk && ra1 < N) ? X[xy_at(ra1, l, ldx)] : 0.0;
+      const double b0 = (lk && cb0 < N) ? Yt[xy_at(cb0, l, ldx)] : 0.0;
+      const double b1 = (lk && cb1 < N) ? Yt[xy_at(cb1, l, ldx)] : 0.0;
+      dmma884(acc[0][0][0], acc[0][0][1], a0, b0);
+      dmma884(acc[0][1][0], acc[0][1][1], a0, b1);
+      dmma884(acc[1][0][0], acc[1][0][1], a1, b0);
+      dmma884(acc[1][1][0], acc[1][1][1], a1, b1);
+    }
+    double old[2][2][2];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int row = r0 + 8 * a + lr, col = c0 + 8 * b + 2 * lc + e;
+          old[a][b][e] = (row < N && col < N) ? G[row + (size_t)col * ldg] : 0.0;
+        }
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int row = r0 + 8 * a + lr, col = c0 + 8 * b + 2 * lc + e;
+          if (row < N && col < N) G[row + (size_t)col * ldg] = -acc[a][b][e] + old[a][b][e];
+        }
+  }
+  __syncthreads();
+}
+
+// G <- G - X Yt^T over the m queued columns: one DMMA rank-m update.
 __device__ __forceinline__ void rank_update(double *G, int ldg, const double *X, const double *Yt,
                                             int N, int ldx, int m) {
   if (N % 24 == 0) flush_tiles<3, 3>(G, ldg, X, Yt, N, ldx, m);
   else if (N % 16 == 0) flush_tiles<2, 2>(G, ldg, X, Yt, N, ldx, m);
-  else blk_dmma(N, N, m, -1.0, MatRef{X, 1, ldx}, false, MatRef{Yt, ldx, 1}, false, 1.0, G, ldg);
+  else flush_generic(G, ldg, X, Yt, N, ldx, m);
 }
 
 // The 2N proposals of one slice (LocalK_prop_L: bonds 2N..1, LocalK_prop_R:
@@ -522,12 +582,9 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
   }
   __syncthreads();
   double *pdat = s.red + 48;      // accepted proposal: Prod(4), D11, D12, det(Prod)
-  // rows p1, p2 of Yt and X of the accepted bond, interleaved per column q
-  // ([q][Yt(p1), Yt(p2), X(p1), X(p2)]), staged by warp 0 after its ballot
-  // so that the column phase reads them as 16-byte pairs
-  const int soff = (7 * N + 1) & ~1;
-  double *stg = s.vec + soff;
-  const bool staged = 4 * k2 <= 8 * N - soff;
+  // column pairs of X and Yt as 16-byte words: pair q / 2 of row i
+  const double2 *X2 = reinterpret_cast<const double2 *>(X);
+  const double2 *Y2 = reinterpret_cast<const double2 *>(Yt);
   const int *__restrict__ bond = s.bond;
   volatile int *flag = s.flag;
   unsigned int st = 0;
@@ -554,14 +611,12 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
       {
         // m is even (two columns per accept): two independent FMA chains
         double h11 = 0.0, h12 = 0.0, h21 = 0.0, h22 = 0.0;
-        const double *xp1 = X + p1, *xp2 = X + p2, *yp1 = Yt + p1, *yp2 = Yt + p2;
 #pragma unroll 2
         for (int q = 0; q < m; q += 2) {
-          const size_t o0 = (size_t)q * ldx, o1 = o0 + ldx;
-          const double xa0 = xp1[o0], xb0 = xp2[o0], ya0 = yp1[o0], yb0 = yp2[o0];
-          const double xa1 = xp1[o1], xb1 = xp2[o1], ya1 = yp1[o1], yb1 = yp2[o1];
-          g11 -= xa0 * ya0; g12 -= xa0 * yb0; g21 -= xb0 * ya0; g22 -= xb0 * yb0;
-          h11 += xa1 * ya1; h12 += xa1 * yb1; h21 += xb1 * ya1; h22 += xb1 * yb1;
+          const size_t o = (size_t)(q >> 1) * ldx;
+          const double2 xa = X2[o + p1], xb = X2[o + p2], ya = Y2[o + p1], yb = Y2[o + p2];
+          g11 -= xa.x * ya.x; g12 -= xa.x * yb.x; g21 -= xb.x * ya.x; g22 -= xb.x * yb.x;
+          h11 += xa.y * ya.y; h12 += xa.y * yb.y; h21 += xb.y * ya.y; h22 += xb.y * yb.y;
         }
         g11 -= h11; g12 -= h12; g21 -= h21; g22 -= h22;
       }
@@ -606,14 +661,7 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
         pdat[4] = D11; pdat[5] = D12; pdat[6] = det;
         flag[1] = b;
       }
-      if (first < 32 && staged) {
-        const int f1 = __shfl_sync(Z2_FULL, p1, first), f2 = __shfl_sync(Z2_FULL, p2, first);
-        for (int q = lane; q < m; q += 32) {
-          const size_t oq = (size_t)q * ldx;
-          double *d = stg + 4 * q;
-          d[0] = Yt[f1 + oq]; d[1] = Yt[f2 + oq]; d[2] = X[f1 + oq]; d[3] = X[f2 + oq];
-        }
-      }
+
       st = ranf_adv(st, cnt);
       rpos += cnt;
       den += cnt;
@@ -641,43 +689,24 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
         {
           // m is even: two independent FMA chains per output
           double w0 = 0.0, w1 = 0.0, z0 = 0.0, z1 = 0.0;
-          const double *xi_ = X + i, *yi_ = Yt + i;
-          if (staged) {
-            const double2 *sp = reinterpret_cast<const double2 *>(stg);
 #pragma unroll 2
-            for (int q = 0; q < m; q += 2) {
-              const size_t o0 = (size_t)q * ldx, o1 = o0 + ldx;
-              const double xa = xi_[o0], ya = yi_[o0], xb = xi_[o1], yb = yi_[o1];
-              const double2 ya0 = sp[2 * q], xa0 = sp[2 * q + 1];
-              const double2 ya1 = sp[2 * q + 2], xa1 = sp[2 * q + 3];
-              const double a1 = ya0.x, a2 = ya0.y, b1 = xa0.x, b2 = xa0.y;
-              const double c1 = ya1.x, c2 = ya1.y, d1 = xa1.x, d2 = xa1.y;
-              u0 -= xa * a1; u1 -= xa * a2; v0 -= b1 * ya; v1 -= b2 * ya;
-              w0 += xb * c1; w1 += xb * c2; z0 += d1 * yb; z1 += d2 * yb;
-            }
-          } else {
-            const double *xp1 = X + p1, *xp2 = X + p2, *yp1 = Yt + p1, *yp2 = Yt + p2;
-#pragma unroll 2
-            for (int q = 0; q < m; q += 2) {
-              const size_t o0 = (size_t)q * ldx, o1 = o0 + ldx;
-              const double xa = xi_[o0], ya = yi_[o0], xb = xi_[o1], yb = yi_[o1];
-              const double a1 = yp1[o0], a2 = yp2[o0], b1 = xp1[o0], b2 = xp2[o0];
-              const double c1 = yp1[o1], c2 = yp2[o1], d1 = xp1[o1], d2 = xp2[o1];
-              u0 -= xa * a1; u1 -= xa * a2; v0 -= b1 * ya; v1 -= b2 * ya;
-              w0 += xb * c1; w1 += xb * c2; z0 += d1 * yb; z1 += d2 * yb;
-            }
+          for (int q = 0; q < m; q += 2) {
+            const size_t o = (size_t)(q >> 1) * ldx;
+            const double2 xr = X2[o + i], yr = Y2[o + i];
+            const double2 y1 = Y2[o + p1], y2 = Y2[o + p2], x1 = X2[o + p1], x2 = X2[o + p2];
+            u0 -= xr.x * y1.x; u1 -= xr.x * y2.x; v0 -= x1.x * yr.x; v1 -= x2.x * yr.x;
+            w0 += xr.y * y1.y; w1 += xr.y * y2.y; z0 += x1.y * yr.y; z1 += x2.y * yr.y;
           }
           u0 -= w0; u1 -= w1; v0 -= z0; v1 -= z1;
         }
         // temp = Uhlp * Prodinv ; Vhlp = Delta (I - G)(P, :)
-        X[i + (size_t)m * ldx] = u0 * q00 + u1 * q10;
-        X[i + (size_t)(m + 1) * ldx] = u0 * q01 + u1 * q11;
+        const size_t om = (size_t)(m >> 1) * ldx + i;
+        reinterpret_cast<double2 *>(X)[om] = make_double2(u0 * q00 + u1 * q10, u0 * q01 + u1 * q11);
         double y0 = -D11 * v0 - D12 * v1;
         double y1 = -D12 * v0 - D11 * v1;
         if (i == p1) { y0 += D11; y1 += D12; }
         if (i == p2) { y0 += D12; y1 += D11; }
-        Yt[i + (size_t)m * ldx] = y0;
-        Yt[i + (size_t)(m + 1) * ldx] = y1;
+        reinterpret_cast<double2 *>(Yt)[om] = make_double2(y0, y1);
       }
       if (threadIdx.x == 0) {
         const signed char sn = (signed char)(-sig[b]);

@@ -322,14 +322,14 @@ __device__ __noinline__ void global_flip_slice(const ChainDesc &c, const Smem &s
   for (int i = threadIdx.x; i < N; i += Z2_NT) {
     const double u0 = G[i + (size_t)p1 * ldg], u1 = G[i + (size_t)p2 * ldg];
     const double v0 = G[p1 + (size_t)i * ldg], v1 = G[p2 + (size_t)i * ldg];
-    X[i] = u0 * q00 + u1 * q10;
-    X[i + ldx] = u0 * q01 + u1 * q11;
+    X[2 * i] = u0 * q00 + u1 * q10;       // columns 0, 1 of the paired layout
+    X[2 * i + 1] = u0 * q01 + u1 * q11;
     double y0 = -D11 * v0 - D12 * v1;
     double y1 = -D12 * v0 - D11 * v1;
     if (i == p1) { y0 += D11; y1 += D12; }
     if (i == p2) { y0 += D12; y1 += D11; }
-    Yt[i] = y0;
-    Yt[i + ldx] = y1;
+    Yt[2 * i] = y0;
+    Yt[2 * i + 1] = y1;
   }
   __syncthreads();
   rank_update(G, ldg, X, Yt, N, ldx, 2);
