@@ -384,7 +384,11 @@ extern "C" int z2_create(z2_handle **out, const z2_chain_params *params, int32_t
     conf_set_host(p, C.N, C.Ltrot, C.sigma0, C.iseed0);
     // shared-memory plan
     const int N = C.N;
-    const int ldg = (N % 2) ? N : N + 1;
+    // leading dimension of G and the QR work matrix in shared memory: N + 2
+    // (= 2 mod 4) when 4 divides N, so the flush's accumulator fragments hit
+    // distinct banks and the checkerboard sweeps move 16-byte pairs; odd
+    // otherwise (conflict-free strided rows)
+    const int ldg = (N % 4 == 0) ? N + 2 : ((N % 2) ? N : N + 1);
     int small = smem_small_bytes(N);
     int k = h->opt.delay_k > 0 ? h->opt.delay_k : default_k(N);
     if (h->opt.delay_k_chain && h->opt.delay_k_chain[c] > 0) k = h->opt.delay_k_chain[c];

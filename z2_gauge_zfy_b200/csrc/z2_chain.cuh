@@ -168,17 +168,33 @@ __device__ __noinline__ void kin_fused(const Smem &s, double *M, size_t vs, size
   const double *__restrict__ tc = s.tc;
   const double *__restrict__ ts = s.ts;
   const int tasks = n * L;
+  // a lattice row of one matrix column is contiguous when ks == 1: with an
+  // even column stride and an aligned matrix it moves as 16-byte pairs
+  const bool pairs = ks == 1 && (vs & 1) == 0 && (reinterpret_cast<size_t>(M) & 15) == 0;
   // groups 0, 1 on lattice rows
   for (int t = threadIdx.x; t < tasks; t += Z2_NT) {
     const int i = t % n, y = t / n;
     double *p = M + (size_t)i * vs + (size_t)(y * L) * ks;
     double v[L];
+    if (pairs) {
 #pragma unroll
-    for (int x = 0; x < L; ++x) v[x] = p[(size_t)x * ks];
+      for (int x = 0; x < L; x += 2) {
+        const double2 w = reinterpret_cast<const double2 *>(p)[x >> 1];
+        v[x] = w.x; v[x + 1] = w.y;
+      }
+    } else {
+#pragma unroll
+      for (int x = 0; x < L; ++x) v[x] = p[(size_t)x * ks];
+    }
     kin_line_odd<L>(v, tc, ts, fl, y * HL, 1);
     kin_line_even<L>(v, tc, ts, fl, H + y * HL, 1);
+    if (pairs) {
 #pragma unroll
-    for (int x = 0; x < L; ++x) p[(size_t)x * ks] = v[x];
+      for (int x = 0; x < L; x += 2) reinterpret_cast<double2 *>(p)[x >> 1] = make_double2(v[x], v[x + 1]);
+    } else {
+#pragma unroll
+      for (int x = 0; x < L; ++x) p[(size_t)x * ks] = v[x];
+    }
   }
   __syncthreads();
   // groups 2, 3, 3, 2 on lattice columns
@@ -201,14 +217,93 @@ __device__ __noinline__ void kin_fused(const Smem &s, double *M, size_t vs, size
     const int i = t % n, y = t / n;
     double *p = M + (size_t)i * vs + (size_t)(y * L) * ks;
     double v[L];
+    if (pairs) {
 #pragma unroll
-    for (int x = 0; x < L; ++x) v[x] = p[(size_t)x * ks];
+      for (int x = 0; x < L; x += 2) {
+        const double2 w = reinterpret_cast<const double2 *>(p)[x >> 1];
+        v[x] = w.x; v[x + 1] = w.y;
+      }
+    } else {
+#pragma unroll
+      for (int x = 0; x < L; ++x) v[x] = p[(size_t)x * ks];
+    }
     kin_line_even<L>(v, tc, ts, fl, H + y * HL, 1);
     kin_line_odd<L>(v, tc, ts, fl, y * HL, 1);
+    if (pairs) {
 #pragma unroll
-    for (int x = 0; x < L; ++x) p[(size_t)x * ks] = v[x];
+      for (int x = 0; x < L; x += 2) reinterpret_cast<double2 *>(p)[x >> 1] = make_double2(v[x], v[x + 1]);
+    } else {
+#pragma unroll
+      for (int x = 0; x < L; ++x) p[(size_t)x * ks] = v[x];
+    }
   }
   __syncthreads();
+}
+
+// kin_fused for M <- M B (vectors are the rows of M, sites stride ld) when ld
+// is even: a thread takes two adjacent rows, so every site moves as one
+// 16-byte pair; the rotations and their order are kin_fused's.
+template <int L>
+__device__ __forceinline__ void kin_pair_odd(double (&v)[L], double (&w)[L], const double *__restrict__ tc,
+                                             const double *__restrict__ ts, double fl, int q0, int qs) {
+#pragma unroll
+  for (int m = 0; m < L / 2; ++m) {
+    const int q = q0 + m * qs;
+    const double C = tc[q], S = fl * ts[q];
+    kin_rot(v[2 * m + 1], v[(2 * m + 2) % L], C, S);
+    kin_rot(w[2 * m + 1], w[(2 * m + 2) % L], C, S);
+  }
+}
+template <int L>
+__device__ __forceinline__ void kin_pair_even(double (&v)[L], double (&w)[L], const double *__restrict__ tc,
+                                              const double *__restrict__ ts, double fl, int q0, int qs) {
+#pragma unroll
+  for (int m = 0; m < L / 2; ++m) {
+    const int q = q0 + m * qs;
+    const double C = tc[q], S = fl * ts[q];
+    kin_rot(v[2 * m], v[2 * m + 1], C, S);
+    kin_rot(w[2 * m], w[2 * m + 1], C, S);
+  }
+}
+template <int L>
+__device__ __noinline__ void kin_fused_rowpairs(const Smem &s, double *M, size_t ld, int n, int nflag) {
+  constexpr int H = L * L / 2, HL = L / 2;
+  const double fl = (double)nflag;
+  const double *__restrict__ tc = s.tc;
+  const double *__restrict__ ts = s.ts;
+  const int n2 = n >> 1, tasks = n2 * L;
+  for (int sweep = 0; sweep < 3; ++sweep) {
+    for (int t = threadIdx.x; t < tasks; t += Z2_NT) {
+      const int i = 2 * (t % n2), line = t / n2;
+      double v[L], w[L];
+      // sweep 0 and 2: lattice row `line` (sites line L + x); sweep 1:
+      // lattice column `line` (sites y L + line)
+      const size_t base = (sweep == 1) ? (size_t)line * ld : (size_t)(line * L) * ld;
+      const size_t step = (sweep == 1) ? (size_t)L * ld : ld;
+      double2 *p = reinterpret_cast<double2 *>(M + i + base);
+      const size_t st2 = step >> 1;
+#pragma unroll
+      for (int x = 0; x < L; ++x) {
+        const double2 u = p[(size_t)x * st2];
+        v[x] = u.x; w[x] = u.y;
+      }
+      if (sweep == 0) {
+        kin_pair_odd<L>(v, w, tc, ts, fl, line * HL, 1);
+        kin_pair_even<L>(v, w, tc, ts, fl, H + line * HL, 1);
+      } else if (sweep == 1) {
+        kin_pair_odd<L>(v, w, tc, ts, fl, 2 * H + line, L);
+        kin_pair_even<L>(v, w, tc, ts, fl, 3 * H + line, L);
+        kin_pair_even<L>(v, w, tc, ts, fl, 3 * H + line, L);
+        kin_pair_odd<L>(v, w, tc, ts, fl, 2 * H + line, L);
+      } else {
+        kin_pair_even<L>(v, w, tc, ts, fl, H + line * HL, 1);
+        kin_pair_odd<L>(v, w, tc, ts, fl, line * HL, 1);
+      }
+#pragma unroll
+      for (int x = 0; x < L; ++x) p[(size_t)x * st2] = make_double2(v[x], w[x]);
+    }
+    __syncthreads();
+  }
 }
 
 // kin_fused for the lattice sizes it is instantiated for; false otherwise.
@@ -242,6 +337,18 @@ __device__ __noinline__ void kin_rows(const ChainDesc &c, const Smem &s, double 
 // row through all eight passes.
 __device__ __noinline__ void kin_cols(const ChainDesc &c, const Smem &s, double *M, int ld, int nrows,
                          int nflag) {
+  if ((ld & 1) == 0 && (nrows & 1) == 0 && (reinterpret_cast<size_t>(M) & 15) == 0) {
+    switch (c.kin_fused) {
+      case 4: kin_fused_rowpairs<4>(s, M, (size_t)ld, nrows, nflag); return;
+      case 6: kin_fused_rowpairs<6>(s, M, (size_t)ld, nrows, nflag); return;
+      case 8: kin_fused_rowpairs<8>(s, M, (size_t)ld, nrows, nflag); return;
+      case 10: kin_fused_rowpairs<10>(s, M, (size_t)ld, nrows, nflag); return;
+      case 12: kin_fused_rowpairs<12>(s, M, (size_t)ld, nrows, nflag); return;
+      case 14: kin_fused_rowpairs<14>(s, M, (size_t)ld, nrows, nflag); return;
+      case 16: kin_fused_rowpairs<16>(s, M, (size_t)ld, nrows, nflag); return;
+      default: break;
+    }
+  }
   if (kin_fused_any(c.kin_fused, s, M, 1, (size_t)ld, nrows, nflag)) return;
   const int half = c.half;
   const double fl = (double)nflag;

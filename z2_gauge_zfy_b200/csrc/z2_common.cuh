@@ -46,7 +46,9 @@ enum { ST_NONFINITE = 1, ST_BADARG = 2 };
 struct ChainDesc {
   // sizes
   int N, Lx, Ly, Ltrot, Nwrap, Nst, nb, half;
-  int ldg;          // odd leading dimension of shared-memory matrices
+  int ldg;          // leading dimension of shared-memory matrices (N + 2 when
+                    // 4 divides N: 16-byte pairs, conflict-free DMMA
+                    // accumulator fragments; else odd)
   int k2;           // 2 * delayed-update rank
   int g_in_smem;    // G (and the QR work matrix) fit in the arena
   int small_bytes;  // bytes of the fixed small region (start of smem)
