@@ -257,6 +257,83 @@ __device__ __noinline__ void blk_org2r_tc(double *A, int lda, int m, int n, cons
   }
 }
 
+// T of one block of reflectors (DLARFT forward / columnwise), by one warp:
+// T is the inverse of the upper-triangular matrix with diagonal 1/tau and
+// strict upper part S = V^T V (DLARFT's column recurrence is exactly the
+// forward substitution of that inverse); diagonal blocks of size b pair up
+// as T12 = -T11 S12 T22, four levels of short dot products instead of 16
+// dependent columns.  A zero tau zeroes its row and column, as in DLARFT.
+// S, T: ib x ib (ld ib); tb: the block's tau; Xs: 4 ib doubles of scratch.
+__device__ __forceinline__ void warp_larft_t(const double *S, double *T, int ib, const double *tb,
+                                             double *Xs) {
+  const int lane = threadIdx.x & 31;
+  for (int e = lane; e < ib * ib; e += 32) {
+    const int r = e % ib, c = e / ib;
+    T[e] = (r == c) ? tb[c] : 0.0;
+  }
+  __syncwarp();
+  for (int b = 1; b < ib; b <<= 1) {
+    const int np = (ib + 2 * b - 1) / (2 * b), bb = b * b;
+    for (int e = lane; e < np * bb; e += 32) {
+      const int p = e / bb, r = (e % bb) % b, c = (e % bb) / b;
+      const int k = 2 * b * p, k2 = k + b;
+      if (k2 + c < ib) {
+        double x0 = 0.0, x1 = 0.0;
+        for (int q = 0; q <= c; q += 2) {
+          x0 += S[(k + r) + (k2 + q) * ib] * T[(k2 + q) + (k2 + c) * ib];
+          if (q + 1 <= c) x1 += S[(k + r) + (k2 + q + 1) * ib] * T[(k2 + q + 1) + (k2 + c) * ib];
+        }
+        Xs[e] = x0 + x1;
+      }
+    }
+    __syncwarp();
+    for (int e = lane; e < np * bb; e += 32) {
+      const int p = e / bb, r = (e % bb) % b, c = (e % bb) / b;
+      const int k = 2 * b * p, k2 = k + b;
+      if (k2 + c < ib) {
+        double t0 = 0.0, t1 = 0.0;
+        for (int q = r; q < b; q += 2) {
+          t0 += T[(k + r) + (k + q) * ib] * Xs[p * bb + q + c * b];
+          if (q + 1 < b) t1 += T[(k + r) + (k + q + 1) * ib] * Xs[p * bb + q + 1 + c * b];
+        }
+        T[(k + r) + (k2 + c) * ib] = -(t0 + t1);
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// S = V^T V (ib x ib, ld ib, ib <= 16) for the unit lower trapezoidal V of
+// the reflectors stored in A(i0:n, i0:i0+ib), by one warp: one 16 x 16 DMMA
+// group over k = n - i0, the operand read from A with the unit diagonal and
+// zero upper part applied (the same k order and values as blk_dmma on a
+// copy of V, so the same bits).
+__device__ __forceinline__ void warp_gram_v(const double *A, int lda, int n, int i0, int ib, double *S) {
+  const int lane = threadIdx.x & 31, lr = lane >> 2, lc = lane & 3;
+  const int mp = n - i0;
+  auto vat = [&](int l, int c) -> double {
+    if (l >= mp || c >= ib) return 0.0;
+    return (l == c) ? 1.0 : (l > c ? A[(i0 + l) + (size_t)(i0 + c) * lda] : 0.0);
+  };
+  double acc[2][2][2] = {};
+  for (int l0 = 0; l0 < mp; l0 += 4) {
+    const double f0 = vat(l0 + lc, lr), f1 = vat(l0 + lc, 8 + lr);
+    dmma884(acc[0][0][0], acc[0][0][1], f0, f0);
+    dmma884(acc[0][1][0], acc[0][1][1], f0, f1);
+    dmma884(acc[1][0][0], acc[1][0][1], f1, f0);
+    dmma884(acc[1][1][0], acc[1][1][1], f1, f1);
+  }
+#pragma unroll
+  for (int u = 0; u < 2; ++u)
+#pragma unroll
+    for (int v = 0; v < 2; ++v)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int r = 8 * u + lr, c = 8 * v + 2 * lc + e;
+        if (r < ib && c < ib) S[r + c * ib] = 1.0 * acc[u][v][e];
+      }
+}
+
 // DORGQR for a square n x n matrix with n reflectors, blocked: blocks of nb
 // reflectors from the last to the first, each applied as the compact WY form
 // H_i0 ... H_i0+ib-1 = I - V T V^T (DLARFT forward/columnwise) by DMMA GEMMs:
@@ -269,7 +346,7 @@ __device__ __noinline__ void blk_org2r_tc(double *A, int lda, int m, int n, cons
 // work.  When work is too small the unblocked DORG2R runs instead (same Q up
 // to rounding).
 __device__ __noinline__ void blk_orgqr(double *A, int lda, int n, const double *tau, double *work,
-                                      int wd, double *small, int sd) {
+                                      int wd, double *small, int sd, double *tscr = nullptr) {
   const int ldv = ((n + 11) & ~15) + 4;
   int nb = 16;
   auto need = [n, ldv, sd](int b) {
@@ -286,6 +363,28 @@ __device__ __noinline__ void blk_orgqr(double *A, int lda, int n, const double *
   double *T = (2 * nb * nb <= sd) ? small : W + (size_t)ldw * (n > nb ? n - nb : 0);
   double *S = T + nb * nb;
   const int tid = threadIdx.x;
+  // Prologue (tscr: nb^2 ceil(n / nb) doubles of global scratch): the T of
+  // every block depends only on that block's reflectors, which the backward
+  // loop below does not touch before the block's turn, so all of them are
+  // formed first, one warp per block in parallel, instead of one after the
+  // other inside the loop.
+  if (tscr != nullptr && wd < Z2_WARPS * (2 * nb * nb + 4 * nb)) tscr = nullptr;
+  if (tscr != nullptr) {
+    const int nblk = (n + nb - 1) / nb, warp = tid >> 5;
+    double *Sw = work + (size_t)warp * (2 * nb * nb + 4 * nb);
+    double *Tw = Sw + nb * nb, *Xw = Tw + nb * nb;
+    for (int bi = warp; bi < nblk; bi += Z2_WARPS) {
+      const int i0 = bi * nb, ib = (n - i0) < nb ? (n - i0) : nb;
+      warp_gram_v(A, lda, n, i0, ib, Sw);
+      __syncwarp();
+      warp_larft_t(Sw, Tw, ib, tau + i0, Xw);
+      __syncwarp();
+      double *td = tscr + (size_t)bi * nb * nb;
+      for (int e = tid & 31; e < ib * ib; e += 32) td[e] = Tw[e];
+      __syncwarp();
+    }
+    __syncthreads();
+  }
   for (int i0 = ((n - 1) / nb) * nb; i0 >= 0; i0 -= nb) {
     const int ib = (n - i0) < nb ? (n - i0) : nb;
     const int mp = n - i0, nc = n - i0 - ib;
@@ -294,53 +393,15 @@ __device__ __noinline__ void blk_orgqr(double *A, int lda, int n, const double *
       for (int r = tid & 31; r < mp; r += 32)
         V[r + (size_t)c * ldv] = (r == c) ? 1.0 : (r > c ? A[(i0 + r) + (size_t)(i0 + c) * lda] : 0.0);
     __syncthreads();
-    // S = V^T V
-    blk_dmma(ib, ib, mp, 1.0, MatRef{V, ldv, 1}, false, MatRef{V, 1, ldv}, false, 0.0, S, ib);
-    // T (DLARFT).  T is the inverse of the upper-triangular matrix with
-    // diagonal 1/tau and strict upper part S (DLARFT's column recurrence is
-    // exactly the forward substitution of that inverse); warp 0 forms it by
-    // doubling: diagonal blocks of size b pair up as T12 = -T11 S12 T22, four
-    // levels of short dot products instead of 16 dependent columns.  A zero
-    // tau zeroes its row and column, as in DLARFT.  Needs 4 nb doubles of
-    // scratch in W; without them the per-row recurrence runs.
-    if (ldw * (n - nb) >= 4 * nb) {
-      double *Xs = W;
-      if (tid < 32) {
-        for (int e = tid; e < ib * ib; e += 32) {
-          const int r = e % ib, c = e / ib;
-          T[e] = (r == c) ? tau[i0 + c] : 0.0;
-        }
-        __syncwarp();
-        for (int b = 1; b < ib; b <<= 1) {
-          const int np = (ib + 2 * b - 1) / (2 * b), bb = b * b;
-          for (int e = tid; e < np * bb; e += 32) {
-            const int p = e / bb, r = (e % bb) % b, c = (e % bb) / b;
-            const int k = 2 * b * p, k2 = k + b;
-            if (k2 + c < ib) {
-              double x0 = 0.0, x1 = 0.0;
-              for (int q = 0; q <= c; q += 2) {
-                x0 += S[(k + r) + (k2 + q) * ib] * T[(k2 + q) + (k2 + c) * ib];
-                if (q + 1 <= c) x1 += S[(k + r) + (k2 + q + 1) * ib] * T[(k2 + q + 1) + (k2 + c) * ib];
-              }
-              Xs[e] = x0 + x1;
-            }
-          }
-          __syncwarp();
-          for (int e = tid; e < np * bb; e += 32) {
-            const int p = e / bb, r = (e % bb) % b, c = (e % bb) / b;
-            const int k = 2 * b * p, k2 = k + b;
-            if (k2 + c < ib) {
-              double t0 = 0.0, t1 = 0.0;
-              for (int q = r; q < b; q += 2) {
-                t0 += T[(k + r) + (k + q) * ib] * Xs[p * bb + q + c * b];
-                if (q + 1 < b) t1 += T[(k + r) + (k + q + 1) * ib] * Xs[p * bb + q + 1 + c * b];
-              }
-              T[(k + r) + (k2 + c) * ib] = -(t0 + t1);
-            }
-          }
-          __syncwarp();
-        }
-      }
+    // S = V^T V (the prologue already folded it into T)
+    if (tscr == nullptr)
+      blk_dmma(ib, ib, mp, 1.0, MatRef{V, ldv, 1}, false, MatRef{V, 1, ldv}, false, 0.0, S, ib);
+    // T (DLARFT): from the prologue when it ran, else by one warp here
+    if (tscr != nullptr) {
+      const double *tsrc = tscr + (size_t)(i0 / nb) * nb * nb;
+      for (int e = tid; e < ib * ib; e += Z2_NT) T[e] = tsrc[e];
+    } else if (ldw * (n - nb) >= 4 * nb) {
+      if (tid < 32) warp_larft_t(S, T, ib, tau + i0, W);
     } else if (tid < ib) {
       const int r = tid;
       double tr[16];

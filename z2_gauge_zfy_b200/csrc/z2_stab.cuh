@@ -24,7 +24,7 @@ __device__ __noinline__ void dev_stab_U(const Smem &s, int N, double *A, int lda
     blk_perm_cols(W0, N, V, N, N, N, jpvt, true);
     blk_dmma(N, N, N, 1.0, MatRef{W0, 1, N}, false, MatRef{A, lda, 1}, true, 0.0, V, N);
   }
-  blk_orgqr(A, lda, N, tau, s.tile, s.tile_doubles, s.vec + 4 * N, 4 * N);   // ZUNGQR
+  blk_orgqr(A, lda, N, tau, s.tile, s.tile_doubles, s.vec + 4 * N, 4 * N, W0);   // ZUNGQR (W0 free)
   blk_copy(U, N, A, lda, N, N);                    // UR = Q, or UL^T = Q
 }
 
@@ -71,7 +71,7 @@ __device__ __noinline__ void dev_stab_green(const Smem &s, int N, int nt, int Lt
   for (int j = threadIdx.x / 32; j < N; j += Z2_WARPS)
     for (int i = threadIdx.x & 31; i <= j; i += 32) W3[i + (size_t)j * N] = M[i + (size_t)j * ldm];
   __syncthreads();
-  blk_orgqr(M, ldm, N, tau, s.tile, s.tile_doubles, s.vec + 4 * N, 4 * N);   // Q in M
+  blk_orgqr(M, ldm, N, tau, s.tile, s.tile_doubles, s.vec + 4 * N, 4 * N, W1);   // Q in M (W1 free)
   if (nt < half + 1) {
     // G = UL^T P R^-1 D^-1 Q^T UR^T
     blk_dmma(N, N, N, 1.0, MatRef{M, ldm, 1}, false, MatRef{UR, N, 1}, false, 0.0, W2, N);
