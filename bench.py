@@ -32,7 +32,7 @@ sys.path.insert(0, ROOT)
 DTAU = 0.1
 # DRAM bytes (read + write) of one step of the 256-chain workload, from one
 # ncu capture of the chain kernel (dram__bytes_read.sum + dram__bytes_write.sum)
-TRAFFIC_BYTES_PER_STEP = 3038375936 + 5325586176
+TRAFFIC_BYTES_PER_STEP = 2995005440 + 5308945664
 
 
 def batched_chains(rank: int = 0, n: int = 256):
