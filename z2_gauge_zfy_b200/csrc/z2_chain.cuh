@@ -533,7 +533,7 @@ __device__ __forceinline__ size_t xy_at(int i, int q, int ldx) {
   return (size_t)(q >> 1) * (2 * ldx) + 2 * i + (q & 1);
 }
 
-// G <- G - X Yt^T over the m queued columns (ld ldx) when 8 TR and 8 TC
+// G <- G - X Yt^T over the m queued columns (paired layout) when 8 TR and 8 TC
 // divide N: each warp owns (8 TR) x (8 TC) blocks of G, reads their old
 // values before its DMMA chain (the load latency overlaps the products) and
 // reuses each X fragment TC times and each Yt fragment TR times.  The k loop
@@ -865,7 +865,7 @@ __device__ __noinline__ void obs_equal(const ChainDesc &c, const Smem &s, int nt
   const int W = 2 * c.Lx - 1;
   // task = (row i, one third of the columns j): the row's density, phase
   // and coordinates stay in registers, the warp's lanes take consecutive
-  // rows (G(i, j) contiguous, G(j, i) at the odd stride, column values
+  // rows (G(i, j) contiguous, G(j, i) at the stride ldg, column values
   // broadcast), and no element needs an index division
   const int J3 = (N + 2) / 3;
   for (int t = threadIdx.x; t < 3 * N; t += Z2_NT) {
