@@ -12,6 +12,9 @@
  *
  * Conventions
  *  - Every call returns an int status (z2_status); z2_last_error() gives text.
+ *    A null handle, a chain index out of range or a null buffer that the call
+ *    must read or write returns Z2_ERR_ARG before any device work; outputs
+ *    documented as optional may be null.  z2_destroy(NULL) does nothing.
  *  - All matrices are real float64, column-major N x N, N = Nlx*Nly (the
  *    reference stores complex(kind=8) but every entry is real).
  *  - sigma is float64 (+1/-1) laid out as the Fortran array sigma(2*N, Ltrot).
@@ -85,12 +88,14 @@ int z2_create(z2_handle **out, const z2_chain_params *params, int32_t nchains,
               const z2_options *opt);
 int z2_destroy(z2_handle *h);
 const char *z2_last_error(const z2_handle *h);
+/* N, Ltrot and Nst (= Ltrot / Nwrap) of one chain; each output is optional. */
 int z2_chain_dims(const z2_handle *h, int32_t chain, int32_t *N, int32_t *Ltrot,
                   int32_t *Nst);
 
 /* ---- configuration I/O: conf_in / conf_out (src/fields.f90:214-309,
  *      509-557).  iseed is the ranf state that continues the chain. ---- */
 int z2_set_config(z2_handle *h, int32_t chain, const double *sigma, int32_t iseed);
+/* sigma and iseed are each optional outputs. */
 int z2_get_config(const z2_handle *h, int32_t chain, double *sigma, int32_t *iseed);
 
 /* ---- Local_sweep%pre (src/local_sweep.f90:87-104) on every chain ---- */
@@ -100,7 +105,7 @@ int z2_pre(z2_handle *h);
  *      bin (runs Dyn%reset/sweep_R, src/dynamics.f90:41-62).  The whole bin
  *      of every chain runs in one persistent launch. ---- */
 int z2_sweep(z2_handle *h, int32_t nsweep, int32_t toggle);
-/* Same as z2_sweep, also returning the device time of the launch (ms). */
+/* Same as z2_sweep, also returning the device time of the launch (ms; optional). */
 int z2_sweep_timed(z2_handle *h, int32_t nsweep, int32_t toggle, float *ms);
 
 /* ---- readback ---- */
@@ -163,12 +168,14 @@ int z2_get_global_stats(const z2_handle *h, int32_t chain, double out[5]);
  * allocates and frees its own probe handles. */
 int z2_tune_delay(const z2_chain_params *params, int32_t nchains, const z2_options *opt,
                   int32_t *k_out);
+/* The first n recorded decisions and ratios of one chain; dec and ratios are
+ * each optional. */
 int z2_get_decisions(const z2_handle *h, int32_t chain, uint8_t *dec,
                      double *ratios, size_t n);
 
 /* ---- adjoint (no reference routine): log|det(1 + B_Ltrot...B_1)| of one
  *      spin sector and its gradient wrt the 2N per-bond hopping amplitudes
- *      and mu, at the chain's current sigma. ---- */
+ *      and mu, at the chain's current sigma; each output is optional. ---- */
 int z2_logdet_grad(z2_handle *h, int32_t chain, double *logdet,
                    double *dlogdet_dt, double *dlogdet_dmu);
 

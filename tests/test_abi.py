@@ -47,3 +47,27 @@ def test_create_rejects_bad_arguments(bad, msg):
     with pytest.raises(Z2Error) as e:
         Z2Batch([Chain(**kw)])
     assert e.value.code == 1 and msg in str(e.value)
+
+
+def test_null_handle_is_an_argument_error():
+    """Every entry point that takes a handle returns Z2_ERR_ARG for a null one
+    before touching the device (so this runs without a GPU); z2_destroy(NULL)
+    is a no-op and z2_last_error(NULL) still returns text."""
+    import ctypes as C
+    lib = _ffi.load()
+    skip = {"z2_create", "z2_tune_delay", "z2_stab_green_noalloc", "z2_last_error",
+            "z2_destroy"}
+    checked = 0
+    for name in _ffi.EXPORTS:
+        if name in skip:
+            continue
+        f = getattr(lib, name)
+        # null for every pointer (handle and buffers), zero for every integer
+        args = [0 if t in (C.c_int32, C.c_size_t) else None for t in f.argtypes]
+        assert f(*args) == 1, name
+        checked += 1
+    assert checked == len(_ffi.EXPORTS) - len(skip)
+    assert lib.z2_destroy(None) == 0
+    assert lib.z2_last_error(None) == b"null handle"
+    assert lib.z2_create(None, None, 1, None) == 1
+    assert lib.z2_tune_delay(None, 1, None, None) == 1

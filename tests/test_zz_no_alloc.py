@@ -68,3 +68,35 @@ def test_noalloc_rejects_oversize():
     rc = lib.z2_stab_green_noalloc(n, 1, 10, dummy, dummy, dummy, dummy, dummy, dummy, dummy,
                                    None)
     assert rc == 1               # Z2_ERR_ARG
+
+
+def _udv(rng, n):
+    U, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    D = np.sort(np.exp(rng.uniform(-4, 4, n)))[::-1].copy()
+    V = np.triu(rng.standard_normal((n, n))) + 3 * np.eye(n)
+    return U, D, V
+
+
+def test_noalloc_at_max_size():
+    """N = 144, the largest size the entry point accepts, on both branches of
+    stab_green, against the handle-based z2_stab_green on the same inputs."""
+    torch = pytest.importorskip("torch")
+    lib = _ffi.load()
+    N = _ffi.Z2_NOALLOC_NMAX
+    ch = Chain(RT=1.0, J=0.5, h=0.5, mu=0.0, Nlx=12, Nly=12, Ltrot=40, beta=4.0, Nwrap=10,
+               seed=4242)
+    assert ch.N == N
+    rng = np.random.default_rng(144)
+    with Z2Batch([ch]) as b:
+        for nt in (10, 30):
+            mats = (*_udv(rng, N), *_udv(rng, N))
+            ref = b.stab_green(0, *mats, nt)
+            d = [_dev(torch, m) for m in mats]
+            G = torch.full((N, N), float("nan"), dtype=torch.float64, device="cuda")
+            rc = lib.z2_stab_green_noalloc(N, nt, ch.Ltrot, *[C.c_void_p(x.data_ptr()) for x in d],
+                                           C.c_void_p(G.data_ptr()), None)
+            assert rc == 0
+            torch.cuda.synchronize()
+            got = G.cpu().numpy().T
+            err = np.max(np.abs(got - ref)) / np.max(np.abs(ref))
+            assert err < RTOL, (nt, err)

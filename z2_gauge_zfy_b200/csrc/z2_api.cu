@@ -7,6 +7,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <initializer_list>
 #include <string>
 #include <vector>
 
@@ -659,6 +660,14 @@ static int check_chain(const z2_handle *h, int chain) {
   return Z2_OK;
 }
 
+// Host buffers an entry point reads or writes must be present; a null one is
+// an argument error, reported before any copy.
+static int check_ptrs(const z2_handle *h, const char *fn, std::initializer_list<const void *> ps) {
+  for (const void *p : ps)
+    if (!p) return set_err(const_cast<z2_handle *>(h), Z2_ERR_ARG, "%s: null buffer", fn);
+  return Z2_OK;
+}
+
 extern "C" int z2_chain_dims(const z2_handle *h, int32_t chain, int32_t *N, int32_t *Ltrot,
                              int32_t *Nst) {
   int r = check_chain(h, chain);
@@ -672,7 +681,7 @@ extern "C" int z2_chain_dims(const z2_handle *h, int32_t chain, int32_t *N, int3
 
 extern "C" int z2_set_config(z2_handle *h, int32_t chain, const double *sigma, int32_t iseed) {
   int r = check_chain(h, chain);
-  if (r) return r;
+  if (r || (r = check_ptrs(h, "z2_set_config", {sigma}))) return r;
   ChainHost &C = h->ch[chain];
   std::vector<signed char> s((size_t)C.nb * C.Ltrot);
   for (size_t i = 0; i < s.size(); ++i) {
@@ -725,7 +734,10 @@ static int launch_chains(z2_handle *h, int op, int nsweep, int toggle, float *ms
       CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
       int r = enqueue_chains(h, op, nsweep, toggle);
       cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
-      if (r) return r;
+      if (r) {
+        if (graph) cudaGraphDestroy(graph);
+        return r;
+      }
       if (e != cudaSuccess) return set_err(h, Z2_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
       e = cudaGraphInstantiate(&exec, graph, 0);
       cudaGraphDestroy(graph);
@@ -772,7 +784,7 @@ extern "C" int z2_sweep(z2_handle *h, int32_t nsweep, int32_t toggle) {
 
 extern "C" int z2_get_green(const z2_handle *h, int32_t chain, double *G) {
   int r = check_chain(h, chain);
-  if (r) return r;
+  if (r || (r = check_ptrs(h, "z2_get_green", {G}))) return r;
   z2_handle *hh = const_cast<z2_handle *>(h);
   const ChainHost &C = h->ch[chain];
   CUDA_TRY(hh, cudaSetDevice(h->device));
@@ -782,7 +794,7 @@ extern "C" int z2_get_green(const z2_handle *h, int32_t chain, double *G) {
 
 extern "C" int z2_get_obs_equal(const z2_handle *h, int32_t chain, double out[Z2_NOBS_EQ]) {
   int r = check_chain(h, chain);
-  if (r) return r;
+  if (r || (r = check_ptrs(h, "z2_get_obs_equal", {out}))) return r;
   z2_handle *hh = const_cast<z2_handle *>(h);
   CUDA_TRY(hh, cudaSetDevice(h->device));
   CUDA_TRY(hh, cudaMemcpy(out, h->ch[chain].d.acc + A_BIN0, sizeof(double) * Z2_NOBS_EQ,
@@ -792,7 +804,7 @@ extern "C" int z2_get_obs_equal(const z2_handle *h, int32_t chain, double out[Z2
 
 extern "C" int z2_get_obs_tau(const z2_handle *h, int32_t chain, double *out) {
   int r = check_chain(h, chain);
-  if (r) return r;
+  if (r || (r = check_ptrs(h, "z2_get_obs_tau", {out}))) return r;
   z2_handle *hh = const_cast<z2_handle *>(h);
   const ChainHost &C = h->ch[chain];
   CUDA_TRY(hh, cudaSetDevice(h->device));
@@ -891,7 +903,7 @@ extern "C" int z2_sweep_global(z2_handle *h, int32_t nglobal) {
 
 extern "C" int z2_get_global_stats(const z2_handle *h, int32_t chain, double out[5]) {
   int r = check_chain(h, chain);
-  if (r) return r;
+  if (r || (r = check_ptrs(h, "z2_get_global_stats", {out}))) return r;
   z2_handle *hh = const_cast<z2_handle *>(h);
   double a[A_COUNT];
   CUDA_TRY(hh, cudaSetDevice(h->device));
@@ -903,7 +915,7 @@ extern "C" int z2_get_global_stats(const z2_handle *h, int32_t chain, double out
 
 extern "C" int z2_get_stats(const z2_handle *h, int32_t chain, double out[Z2_NSTATS]) {
   int r = check_chain(h, chain);
-  if (r) return r;
+  if (r || (r = check_ptrs(h, "z2_get_stats", {out}))) return r;
   z2_handle *hh = const_cast<z2_handle *>(h);
   double a[A_COUNT];
   CUDA_TRY(hh, cudaSetDevice(h->device));
@@ -918,7 +930,7 @@ extern "C" int z2_get_stats(const z2_handle *h, int32_t chain, double out[Z2_NST
 
 extern "C" int z2_get_phase_cycles(const z2_handle *h, int32_t chain, double out[Z2_NPHASE]) {
   int r = check_chain(h, chain);
-  if (r) return r;
+  if (r || (r = check_ptrs(h, "z2_get_phase_cycles", {out}))) return r;
   z2_handle *hh = const_cast<z2_handle *>(h);
   CUDA_TRY(hh, cudaSetDevice(h->device));
   CUDA_TRY(hh, cudaMemcpy(out, h->ch[chain].d.acc + A_PH0, sizeof(double) * Z2_NPHASE,
@@ -1016,6 +1028,7 @@ static int upload_desc(z2_handle *h, int chain) {
 extern "C" int z2_set_replay(z2_handle *h, int32_t chain, const double *rr, size_t n) {
   int r = check_chain(h, chain);
   if (r) return r;
+  if (n > 0 && !rr) return set_err(h, Z2_ERR_ARG, "z2_set_replay: null buffer with n = %zu", n);
   ChainHost &C = h->ch[chain];
   CUDA_TRY(h, cudaSetDevice(h->device));
   if (C.replay) { cudaFree(C.replay); C.replay = nullptr; }
@@ -1091,6 +1104,7 @@ static int run_unit(z2_handle *h, int chain, int op, const UnitArgs &a) {
 static int mmult(z2_handle *h, int chain, double *M, int nt, int nflag, int op) {
   int r = check_chain(h, chain);
   if (r) return r;
+  if ((r = check_ptrs(h, "z2_opk_mmult", {M}))) return r;
   ChainHost &C = h->ch[chain];
   if (nt < 1 || nt > C.Ltrot) return set_err(h, Z2_ERR_ARG, "nt = %d out of 1..Ltrot", nt);
   if (nflag != 1 && nflag != -1) return set_err(h, Z2_ERR_ARG, "incorrect nflag %d", nflag);
@@ -1119,7 +1133,7 @@ static void transpose_host(const double *src, double *dst, int N) {
 
 static int stab_u(z2_handle *h, int chain, double *U, double *D, double *V, bool left) {
   int r = check_chain(h, chain);
-  if (r) return r;
+  if (r || (r = check_ptrs(h, left ? "z2_stab_UL" : "z2_stab_UR", {U, D, V}))) return r;
   ChainHost &C = h->ch[chain];
   const int N = C.N;
   const size_t NN = (size_t)N * N;
@@ -1173,7 +1187,7 @@ extern "C" int z2_stab_green(z2_handle *h, int32_t chain, const double *UR, cons
                              const double *VR, const double *UL, const double *DL,
                              const double *VL, int32_t nt, double *G) {
   int r = check_chain(h, chain);
-  if (r) return r;
+  if (r || (r = check_ptrs(h, "z2_stab_green", {UR, DR, VR, UL, DL, VL, G}))) return r;
   ChainHost &C = h->ch[chain];
   const int N = C.N;
   const size_t NN = (size_t)N * N;
@@ -1193,7 +1207,9 @@ extern "C" int z2_stab_green_big(z2_handle *h, int32_t chain, const double *UR, 
                                  const double *VL, double *G00, double *G0t, double *Gt0,
                                  double *Gtt) {
   int r = check_chain(h, chain);
-  if (r) return r;
+  if (r || (r = check_ptrs(h, "z2_stab_green_big",
+                           {UR, DR, VR, UL, DL, VL, G00, G0t, Gt0, Gtt})))
+    return r;
   ChainHost &C = h->ch[chain];
   const int N = C.N;
   const size_t NN = (size_t)N * N;
@@ -1226,6 +1242,13 @@ extern "C" int z2_stab_green_big(z2_handle *h, int32_t chain, const double *UR, 
 
 static __device__ __align__(256) double z2_noalloc_scratch[5 * Z2_NOALLOC_NMAX * Z2_NOALLOC_NMAX];
 
+// Shared work space of the two QR steps, enough for every N <= 144 so that
+// this kernel runs the same QR code as z2_stab_green: the register-resident
+// pivoted QR needs 2N doubles, the blocked DORGQR (16-column blocks) its V and
+// W panels (4544 doubles at N = 144) and, for the T prologue, 8 warps x
+// (2 * 16^2 + 4 * 16) = 4608 doubles.
+constexpr int kNoallocTile = Z2_WARPS * (2 * 16 * 16 + 4 * 16);
+
 __global__ void __launch_bounds__(Z2_NT, 1)
 z2_stab_green_noalloc_kernel(int N, int nt, int Ltrot, const double *UR, const double *DR,
                              const double *VR, const double *UL, const double *DL,
@@ -1239,6 +1262,7 @@ z2_stab_green_noalloc_kernel(int N, int nt, int Ltrot, const double *UR, const d
   s.flag = (int *)(z2_smem + off); off += sizeof(int) * 16;
   off = align16(off);
   s.tile = (double *)(z2_smem + off);
+  s.tile_doubles = kNoallocTile;
   // scratch: M (QR work matrix), W1, W2, W3, UL^T; every entry read is
   // written first by this call, so nothing has to start at zero.
   const size_t NN = (size_t)N * N;
@@ -1247,13 +1271,13 @@ z2_stab_green_noalloc_kernel(int N, int nt, int Ltrot, const double *UR, const d
   dev_stab_green(s, N, nt, Ltrot, UR, DR, VR, ULT, DL, VL, M, N, W1, W2, W3, G);
 }
 
-static size_t noalloc_smem_bytes(int N) {
-  size_t off = sizeof(double) * Z2_NRED + sizeof(double) * 8 * (size_t)N;
-  off += ((sizeof(int) * 2 * (size_t)N) + 15) & ~size_t(15);
-  off += sizeof(int) * 16;
-  off = (off + 15) & ~size_t(15);
-  return off + sizeof(double) * kGemmTile;
+static constexpr size_t noalloc_smem_bytes(int N) {
+  return ((((sizeof(double) * Z2_NRED + sizeof(double) * 8 * (size_t)N) +
+            (((sizeof(int) * 2 * (size_t)N) + 15) & ~size_t(15)) + sizeof(int) * 16) + 15) &
+          ~size_t(15)) + sizeof(double) * kNoallocTile;
 }
+// within the 48 KB a launch gets without opting in to more
+static_assert(noalloc_smem_bytes(Z2_NOALLOC_NMAX) <= 48 * 1024, "no-alloc shared memory");
 
 extern "C" int z2_stab_green_noalloc(int32_t N, int32_t nt, int32_t Ltrot, const double *UR,
                                      const double *DR, const double *VR, const double *UL,
