@@ -71,3 +71,38 @@ def test_null_handle_is_an_argument_error():
     assert lib.z2_last_error(None) == b"null handle"
     assert lib.z2_create(None, None, 1, None) == 1
     assert lib.z2_tune_delay(None, 1, None, None) == 1
+
+
+def _header_arity():
+    txt = open(os.path.join(ROOT, "include", "z2dqmc.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    out = {}
+    for m in re.finditer(r"\b(z2_[a-zA-Z0-9_]+)\s*\(([^;{]*?)\)\s*;", txt):
+        args = m.group(2).strip()
+        out[m.group(1)] = 0 if args in ("", "void") else args.count(",") + 1
+    return out
+
+
+def test_fortran_binding_matches_header():
+    """INTEGRATION.md's ISO_C_BINDING module binds every entry point of the
+    header, each with the header's number of arguments."""
+    txt = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    txt = re.sub(r"&\s*\n\s*", " ", txt)           # join continuation lines
+    fort = {}
+    for m in re.finditer(r"function\s+(z2_[a-z0-9_]+)\s*\(([^)]*)\)\s*bind\(C,\s*name=\"(\w+)\"\)",
+                         txt, flags=re.I):
+        assert m.group(1).lower() == m.group(3).lower()
+        args = m.group(2).strip()
+        fort[m.group(3)] = 0 if not args else args.count(",") + 1
+    hdr = _header_arity()
+    assert sorted(hdr) == sorted(_ffi.EXPORTS)
+    assert sorted(fort) == sorted(hdr)
+    for name, n in hdr.items():
+        assert fort[name] == n, (name, fort[name], n)
+
+
+def test_ctypes_signatures_match_header():
+    """The ctypes declarations carry the header's number of arguments."""
+    lib = _ffi.load()
+    for name, n in _header_arity().items():
+        assert len(getattr(lib, name).argtypes) == n, name
