@@ -25,6 +25,7 @@
 #include <cstring>
 #include <fstream>
 #include <sstream>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -65,14 +66,18 @@ bool read_params(const std::string &path, Params &p) {
   if (lines.size() < 8) return false;
   auto D = [&](int l, int k) { return std::atof(lines[l].at(k).c_str()); };
   auto I = [&](int l, int k) { return std::atoi(lines[l].at(k).c_str()); };
-  p.RT = D(0, 0); p.J = D(0, 1); p.h = D(0, 2); p.mu = D(0, 3); p.Q = D(0, 4);
-  p.Nlx = I(1, 0); p.Nly = I(1, 1); p.Ltrot = I(1, 2); p.beta = D(1, 3);
-  p.NlxT = I(2, 0); p.NlyT = I(2, 1); p.LtrotT = I(2, 2);
-  p.Nwrap = I(3, 0); p.Nbin = I(3, 1); p.Nsweep = I(3, 2);
-  p.is_tau = logical(lines[4][0]); p.Nthermal = I(4, 1);
-  p.is_warm = logical(lines[5][0]); p.Nwarm = I(5, 1);
-  p.is_global = logical(lines[6][0]); p.Nglobal = I(6, 1);
-  p.absolute = I(7, 0);
+  try {   // a line with too few fields is a file that cannot be read
+    p.RT = D(0, 0); p.J = D(0, 1); p.h = D(0, 2); p.mu = D(0, 3); p.Q = D(0, 4);
+    p.Nlx = I(1, 0); p.Nly = I(1, 1); p.Ltrot = I(1, 2); p.beta = D(1, 3);
+    p.NlxT = I(2, 0); p.NlyT = I(2, 1); p.LtrotT = I(2, 2);
+    p.Nwrap = I(3, 0); p.Nbin = I(3, 1); p.Nsweep = I(3, 2);
+    p.is_tau = logical(lines[4][0]); p.Nthermal = I(4, 1);
+    p.is_warm = logical(lines[5][0]); p.Nwarm = I(5, 1);
+    p.is_global = logical(lines[6][0]); p.Nglobal = I(6, 1);
+    p.absolute = I(7, 0);
+  } catch (const std::out_of_range &) {
+    return false;
+  }
   return true;
 }
 
@@ -184,13 +189,13 @@ struct KOut {
   }
 };
 
-static void write_obs_tau_k(z2_handle *h, const std::string &dir, const Params &p, int nch,
-                            const std::vector<double> &tau_real) {
+static int write_obs_tau_k(z2_handle *h, const std::string &dir, const Params &p, int nch,
+                           const std::vector<double> &tau_real) {
   const int N = p.Nlx * p.Nly, Lt = p.Ltrot;
   const size_t n = (size_t)7 * Lt * N;
   std::vector<double> re(n), im(n), sr(n, 0.0), si(n, 0.0);
   for (int c = 0; c < nch; ++c) {
-    if (z2_get_obs_tau_k(h, c, re.data(), im.data())) return;
+    if (int r = z2_get_obs_tau_k(h, c, re.data(), im.data())) return r;
     for (size_t i = 0; i < n; ++i) { sr[i] += re[i] / nch; si[i] += im[i] / nch; }
   }
   const KOut o{dir, N, Lt, p.Nlx, p.Nly, p.beta / Lt, p.beta};
@@ -264,6 +269,7 @@ static void write_obs_tau_k(z2_handle *h, const std::string &dir, const Params &
     o.reciprocal(pr[w][1], g);
     o.at_k(pr[w][2], g, kzero);
   }
+  return Z2_OK;
 }
 
 int fail(z2_handle *h, const char *what, int code) {
@@ -287,6 +293,13 @@ int main(int argc, char **argv) {
     std::fprintf(stderr, "cannot read %s/paramC_sets.txt\n", dir.c_str());
     return 1;
   }
+  // the sizes that conf_transfer's tiling and the stabilization divide by
+  if (p.Nlx < 1 || p.Nly < 1 || p.Ltrot < 1 || p.NlxT < 1 || p.NlyT < 1 || p.LtrotT < 1 ||
+      p.Nwrap < 1 || p.Nsweep < 1 || p.Nbin < 0) {
+    std::fprintf(stderr, "paramC_sets.txt: lattice sizes, Ltrot, Nwrap and Nsweep must be >= 1\n");
+    return 1;
+  }
+  if (nch < 1) { std::fprintf(stderr, "--chains must be >= 1\n"); return 1; }
   if (p.Ltrot % p.Nwrap) { std::fprintf(stderr, "Ltrot must be a multiple of Nwrap\n"); return 1; }
   const int N = p.Nlx * p.Nly, nb = 2 * N;
   // initial configurations (conf_therm_in, src/fields.f90:227-309)
@@ -321,15 +334,19 @@ int main(int argc, char **argv) {
       }
     }
   }
+  // every output file goes to dir: one that cannot be written is an error
+  // here, not lost output later
   FILE *info = std::fopen((dir + "/info.txt").c_str(), "w");
-  if (info) {
-    std::fprintf(info, " ==============================================\n");
-    std::fprintf(info, " Lx %d Ly %d RT %.17g J %.17g h %.17g mu %.17g Q %.17g absolute %d\n", p.Nlx,
-                 p.Nly, p.RT, p.J, p.h, p.mu, p.Q, p.absolute);
-    std::fprintf(info, " Beta %.17g Ltrot %d Dtau %.17g Nwrap %d Nbin %d Nsweep %d chains %d\n",
-                 p.beta, p.Ltrot, p.beta / p.Ltrot, p.Nwrap, p.Nbin, p.Nsweep, nch);
-    std::fprintf(info, " ==============================================\n");
+  if (!info) {
+    std::fprintf(stderr, "cannot write %s/info.txt\n", dir.c_str());
+    return 1;
   }
+  std::fprintf(info, " ==============================================\n");
+  std::fprintf(info, " Lx %d Ly %d RT %.17g J %.17g h %.17g mu %.17g Q %.17g absolute %d\n", p.Nlx,
+               p.Nly, p.RT, p.J, p.h, p.mu, p.Q, p.absolute);
+  std::fprintf(info, " Beta %.17g Ltrot %d Dtau %.17g Nwrap %d Nbin %d Nsweep %d chains %d\n",
+               p.beta, p.Ltrot, p.beta / p.Ltrot, p.Nwrap, p.Nbin, p.Nsweep, nch);
+  std::fprintf(info, " ==============================================\n");
   std::vector<z2_chain_params> cp(nch);
   for (int c = 0; c < nch; ++c)
     cp[c] = z2_chain_params{p.RT, p.J, p.h, p.mu, p.Q, p.Nlx, p.Nly, p.Ltrot, p.beta,
@@ -351,7 +368,7 @@ int main(int argc, char **argv) {
     if ((r = z2_therm(h, p.Nwarm, wacc.data()))) return fail(h, "z2_therm", r);
     double acc = 0.0;
     for (double a : wacc) acc += a / nch;
-    if (info) std::fprintf(info, " Thermalize Accept Ratio : %.17g\n", acc);
+    std::fprintf(info, " Thermalize Accept Ratio : %.17g\n", acc);
   }
   if ((r = z2_pre(h))) return fail(h, "z2_pre", r);
   const char *names[7] = {"flux_avg", "chi_flux", "pair_sc_q0", "cdw_pi", "cdw_shift", "cdw_ratio", "density"};
@@ -363,27 +380,35 @@ int main(int argc, char **argv) {
     double mean[7] = {0};
     for (int c = 0; c < nch; ++c) {
       double o[Z2_NOBS_EQ];
-      z2_get_obs_equal(h, c, o);
+      if ((r = z2_get_obs_equal(h, c, o))) return fail(h, "z2_get_obs_equal", r);
       for (int q = 0; q < 7; ++q) mean[q] += o[q] / nch;
     }
     for (int q = 0; q < 7; ++q) if (q != 4) append(dir, names[q], mean[q]);
     if (istau) {   // raw time-displaced correlators, averaged over chains
       tau_sum.assign(tau.size(), 0.0);
       for (int c = 0; c < nch; ++c) {
-        z2_get_obs_tau(h, c, tau.data());
+        if ((r = z2_get_obs_tau(h, c, tau.data()))) return fail(h, "z2_get_obs_tau", r);
         for (size_t i = 0; i < tau.size(); ++i) tau_sum[i] += tau[i] / nch;
       }
       FILE *f = std::fopen((dir + "/obs_tau_raw").c_str(), "a");
       if (f) { for (double v : tau_sum) std::fprintf(f, " %25.17E\n", v); std::fclose(f); }
-      write_obs_tau_k(h, dir, p, nch, tau_sum);
+      if ((r = write_obs_tau_k(h, dir, p, nch, tau_sum))) return fail(h, "z2_get_obs_tau_k", r);
     }
-    if (nbc % 20 == 0 && info) {
+    if (nbc % 20 == 0) {
       double acc = 0;
-      for (int c = 0; c < nch; ++c) { double st[Z2_NSTATS]; z2_get_stats(h, c, st); acc += st[0]; }
+      for (int c = 0; c < nch; ++c) {
+        double st[Z2_NSTATS];
+        if ((r = z2_get_stats(h, c, st))) return fail(h, "z2_get_stats", r);
+        acc += st[0];
+      }
       std::fprintf(info, " Progress %d : Accept_Klocal_shift: %.17g\n", nbc, acc / (nch * nbc));
       if (p.is_global) {
         double ga = 0;
-        for (int c = 0; c < nch; ++c) { double g[5]; z2_get_global_stats(h, c, g); ga += g[0]; }
+        for (int c = 0; c < nch; ++c) {
+          double g[5];
+          if ((r = z2_get_global_stats(h, c, g))) return fail(h, "z2_get_global_stats", r);
+          ga += g[0];
+        }
         std::fprintf(info, " Progress %d : Accept_Kglobal: %.17g\n", nbc, ga / (nch * nbc));
       }
     }
@@ -391,35 +416,42 @@ int main(int argc, char **argv) {
   double acc = 0, xmax = 0, xmean = 0;
   for (int c = 0; c < nch; ++c) {
     double st[Z2_NSTATS];
-    z2_get_stats(h, c, st);
+    if ((r = z2_get_stats(h, c, st))) return fail(h, "z2_get_stats", r);
     acc += st[0]; xmax = std::max(xmax, st[1]); xmean += st[2];
   }
   const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-  if (info) {
-    if (p.is_global) {   // Global_control_print (src/global_update.f90:339-354)
-      double ga = 0, gs = 0;
-      for (int c = 0; c < nch; ++c) { double g[5]; z2_get_global_stats(h, c, g); ga += g[0]; gs += g[1]; }
-      std::fprintf(info, " Average size of Wolff cluster : %.17g\n", gs / (nch * p.Nbin));
-      std::fprintf(info, " Accept_Kglobal                : %.17g\n", ga / (nch * p.Nbin));
+  if (p.is_global) {   // Global_control_print (src/global_update.f90:339-354)
+    double ga = 0, gs = 0;
+    for (int c = 0; c < nch; ++c) {
+      double g[5];
+      if ((r = z2_get_global_stats(h, c, g))) return fail(h, "z2_get_global_stats", r);
+      ga += g[0];
+      gs += g[1];
     }
-    std::fprintf(info, " Accept_Klocal_shift : %.17g\n", acc / (nch * p.Nbin));
-    std::fprintf(info, " Max diff Matrix     : %.17g\n", xmax);
-    std::fprintf(info, " Mean diff Matrix    : %.17g\n",
-                 xmean / (2.0 * nch * p.Nbin * (p.Ltrot / p.Nwrap) * p.Nsweep));
-    std::fprintf(info, " Tot CPU time        : %.10g\n", secs);
-    std::fclose(info);
+    std::fprintf(info, " Average size of Wolff cluster : %.17g\n", gs / (nch * p.Nbin));
+    std::fprintf(info, " Accept_Kglobal                : %.17g\n", ga / (nch * p.Nbin));
   }
+  std::fprintf(info, " Accept_Klocal_shift : %.17g\n", acc / (nch * p.Nbin));
+  std::fprintf(info, " Max diff Matrix     : %.17g\n", xmax);
+  std::fprintf(info, " Mean diff Matrix    : %.17g\n",
+               xmean / (2.0 * nch * p.Nbin * (p.Ltrot / p.Nwrap) * p.Nsweep));
+  std::fprintf(info, " Tot CPU time        : %.10g\n", secs);
+  std::fclose(info);
   // conf_out (src/fields.f90:509-557)
   FILE *co = std::fopen((dir + "/confout.txt").c_str(), "w");
-  for (int c = 0; c < nch && co; ++c) {
+  if (!co) {
+    std::fprintf(stderr, "cannot write %s/confout.txt\n", dir.c_str());
+    return 1;
+  }
+  for (int c = 0; c < nch; ++c) {
     std::vector<double> s((size_t)nb * p.Ltrot);
     int32_t is = 0;
-    z2_get_config(h, c, s.data(), &is);
+    if ((r = z2_get_config(h, c, s.data(), &is))) return fail(h, "z2_get_config", r);
     std::fprintf(co, " %d\n", is);
     for (double v : s) std::fprintf(co, " %.1f\n", v);
     for (int i = 0; i < N; ++i) std::fprintf(co, " 1.0\n");
   }
-  if (co) std::fclose(co);
+  std::fclose(co);
   z2_destroy(h);
   return 0;
 }
