@@ -37,6 +37,7 @@ def test_no_fallback_without_library(monkeypatch, tmp_path):
     (dict(Ltrot=25, Nwrap=10), "multiple of Nwrap"),
     (dict(absolute=7), "absolute"),
     (dict(beta=0.0), "beta"),
+    (dict(rt_bond=[1.0] * 5), "rt_bond"),
 ])
 def test_create_rejects_bad_arguments(bad, msg):
     """Argument errors (the reference would print and stop) come back as
@@ -47,6 +48,14 @@ def test_create_rejects_bad_arguments(bad, msg):
     with pytest.raises(Z2Error) as e:
         Z2Batch([Chain(**kw)])
     assert e.value.code == 1 and msg in str(e.value)
+
+
+def test_create_rejects_wrong_delay_list():
+    """One delayed-update rank per chain, checked before any device work."""
+    from z2_gauge_zfy_b200 import Chain, Z2Batch, Z2Error
+    with pytest.raises(Z2Error) as e:
+        Z2Batch([Chain()], delay_k_chain=[4, 4])
+    assert e.value.code == 1 and "delay_k_chain" in str(e.value)
 
 
 def test_null_handle_is_an_argument_error():

@@ -44,3 +44,28 @@ def test_null_buffers_rejected_and_handle_survives():
         assert np.array_equal(b.green(0), g0)
         b.sweep(1)
         assert np.all(np.isfinite(b.green(0)))
+
+
+def test_python_mirrors_check_shapes():
+    """The Python mirrors reject arrays whose shape does not match the chain
+    (the library copies exactly N x N or 2N x Ltrot values)."""
+    from z2_gauge_zfy_b200 import Z2Error
+    ch = Chain(RT=1.0, Nlx=4, Nly=4, Ltrot=20, beta=2.0, Nwrap=10, seed=777)
+    N = ch.N
+    eye, one = np.eye(N), np.ones(N)
+    small = np.eye(N - 2)
+    with Z2Batch([ch]) as b:
+        bad = [
+            lambda: b.opk_mmult_R(0, np.ones((N, N - 1)), 1, 1),
+            lambda: b.opk_mmult_L(0, small, 1, 1),
+            lambda: b.stab_UR(0, eye, np.ones(N - 1), eye),
+            lambda: b.stab_green(0, eye, one, eye, small, one, eye, 1),
+            lambda: b.stab_green_big(0, eye, one, eye, eye, one, small),
+            lambda: b.set_config(0, np.ones((ch.Ltrot, 2 * N)), 1),
+        ]
+        for i, call in enumerate(bad):
+            with pytest.raises(Z2Error) as e:
+                call()
+            assert e.value.code == 1 and "needs" in str(e.value), i
+        # the right shapes still go through
+        assert b.opk_mmult_R(0, eye, 1, 1).shape == (N, N)

@@ -90,7 +90,9 @@ def _params(chains):
         p.Nwrap, p.absolute, p.seed = ch.Nwrap, ch.absolute, ch.seed
         if ch.rt_bond is not None:
             rb = np.ascontiguousarray(ch.rt_bond, dtype=np.float64)
-            assert rb.shape == (2 * ch.N,)
+            if rb.shape != (2 * ch.N,):
+                raise Z2Error(1, f"chain {i}: rt_bond has shape {rb.shape}, "
+                                 f"needs one hopping per bond ({2 * ch.N},)")
             keep.append(rb)
             p.rt_bond = dptr(rb)
         else:
@@ -133,7 +135,9 @@ class Z2Batch:
         kc_ptr = None
         if delay_k_chain is not None:
             self._kc = np.ascontiguousarray(delay_k_chain, dtype=np.int32)
-            assert self._kc.shape == (n,)
+            if self._kc.shape != (n,):
+                raise Z2Error(1, f"delay_k_chain has shape {self._kc.shape}, "
+                                 f"needs one rank per chain ({n},)")
             kc_ptr = self._kc.ctypes.data_as(C.POINTER(C.c_int32))
         opt = Options(delay_k, 1 if record else 0, device, 1 if tau else 0, 1 if graph else 0,
                       kc_ptr)
@@ -183,6 +187,26 @@ class Z2Batch:
         return float(ms.value)
 
     # -- configuration -------------------------------------------------------
+    def _shaped(self, chain: int, name: str, a, shape: tuple) -> np.ndarray:
+        """``a`` as float64 if it has ``shape`` (the library copies exactly
+        that many values for this chain), else an argument error."""
+        a = np.asarray(a, dtype=np.float64)
+        if a.shape != shape:
+            raise Z2Error(1, f"{name}: shape {a.shape}, chain {chain} needs {shape}")
+        return a
+
+    def _mats(self, chain: int, **arrays) -> list:
+        """N x N matrices and length-N vectors (names starting with D) of one
+        chain, checked and in the library's layout."""
+        N = self.dims(chain)[0]
+        out = []
+        for name, a in arrays.items():
+            if name.startswith("D"):
+                out.append(np.ascontiguousarray(self._shaped(chain, name, a, (N,))))
+            else:
+                out.append(fmat(self._shaped(chain, name, a, (N, N))).ravel())
+        return out
+
     def dims(self, chain: int):
         N, L, S = C.c_int32(), C.c_int32(), C.c_int32()
         self._c(self.lib.z2_chain_dims(self.h, chain, C.byref(N), C.byref(L), C.byref(S)))
@@ -198,7 +222,8 @@ class Z2Batch:
 
     def set_config(self, chain: int, sigma, iseed: int):
         """Load sigma(2N, Ltrot) and the ranf state (``conf_in``)."""
-        s = fmat(sigma).ravel()
+        N, L, _ = self.dims(chain)
+        s = fmat(self._shaped(chain, "sigma", sigma, (2 * N, L))).ravel()
         self._c(self.lib.z2_set_config(self.h, chain, dptr(s), int(iseed)))
 
     # -- readback ------------------------------------------------------------
@@ -285,22 +310,22 @@ class Z2Batch:
     # -- module-level mirrors --------------------------------------------------
     def opk_mmult_R(self, chain: int, M, nt: int, nflag: int) -> np.ndarray:
         """B_nt^nflag M (``OperatorKin%mmult_R``), nt = 1..Ltrot."""
-        b = fmat(M).ravel()
+        (b,) = self._mats(chain, M=M)
         self._c(self.lib.z2_opk_mmult_R(self.h, chain, dptr(b), nt, nflag))
         n = int(round(np.sqrt(b.size)))
         return b.reshape(n, n).T.copy()
 
     def opk_mmult_L(self, chain: int, M, nt: int, nflag: int) -> np.ndarray:
         """M B_nt^nflag (``OperatorKin%mmult_L``)."""
-        b = fmat(M).ravel()
+        (b,) = self._mats(chain, M=M)
         self._c(self.lib.z2_opk_mmult_L(self.h, chain, dptr(b), nt, nflag))
         n = int(round(np.sqrt(b.size)))
         return b.reshape(n, n).T.copy()
 
     def _stab_u(self, fn, chain, U, D, V):
-        n = U.shape[0]
-        u, v = fmat(U).ravel(), fmat(V).ravel()
-        d = np.ascontiguousarray(D, dtype=np.float64).copy()
+        u, d, v = self._mats(chain, U=U, D=D, V=V)
+        n = d.size
+        d = d.copy()
         self._c(fn(self.h, chain, dptr(u), dptr(d), dptr(v)))
         return u.reshape(n, n).T.copy(), d, v.reshape(n, n).T.copy()
 
@@ -313,18 +338,16 @@ class Z2Batch:
         return self._stab_u(self.lib.z2_stab_UL, chain, U, D, V)
 
     def stab_green(self, chain, UR, DR, VR, UL, DL, VL, nt: int) -> np.ndarray:
-        n = UR.shape[0]
+        args = self._mats(chain, UR=UR, DR=DR, VR=VR, UL=UL, DL=DL, VL=VL)
+        n = args[1].size
         g = np.empty(n * n)
-        args = [fmat(UR).ravel(), np.ascontiguousarray(DR, dtype=np.float64), fmat(VR).ravel(),
-                fmat(UL).ravel(), np.ascontiguousarray(DL, dtype=np.float64), fmat(VL).ravel()]
         self._c(self.lib.z2_stab_green(self.h, chain, *[dptr(a) for a in args], nt, dptr(g)))
         return g.reshape(n, n).T.copy()
 
     def stab_green_big(self, chain, UR, DR, VR, UL, DL, VL):
-        n = UR.shape[0]
+        args = self._mats(chain, UR=UR, DR=DR, VR=VR, UL=UL, DL=DL, VL=VL)
+        n = args[1].size
         outs = [np.empty(n * n) for _ in range(4)]
-        args = [fmat(UR).ravel(), np.ascontiguousarray(DR, dtype=np.float64), fmat(VR).ravel(),
-                fmat(UL).ravel(), np.ascontiguousarray(DL, dtype=np.float64), fmat(VL).ravel()]
         self._c(self.lib.z2_stab_green_big(self.h, chain, *[dptr(a) for a in args],
                                            *[dptr(o) for o in outs]))
         return tuple(o.reshape(n, n).T.copy() for o in outs)
