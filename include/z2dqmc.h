@@ -83,7 +83,10 @@ typedef struct z2_handle z2_handle;
 /* ---- life cycle: Model_init + Prop/WrapList make + Stabilize_init
  *      (src/model.f90:16-36, src/process_matrix.f90:46-112,
  *       src/stabilization.f90:20-32); the initial sigma follows conf_set +
- *      conf_transfer (src/fields.f90:311-507) from each chain's seed. ---- */
+ *      conf_transfer (src/fields.f90:311-507) from each chain's seed.
+ *      Unless out or params is NULL or nchains < 1, *out receives a handle
+ *      even when the call fails: z2_last_error() on it says why, and
+ *      z2_destroy() releases it. ---- */
 int z2_create(z2_handle **out, const z2_chain_params *params, int32_t nchains,
               const z2_options *opt);
 int z2_destroy(z2_handle *h);
