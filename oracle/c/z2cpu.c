@@ -14,8 +14,9 @@
  * the two bit-identical spin sectors and real arithmetic (the reference
  * repeats every step for PropU and PropD in complex(kind=8)).
  *
- * Parity status: parity unpinned against the reference (which cannot be
- * built here); cross-checked against the NumPy oracle (tests/test_cpu_port.py).
+ * Parity status: cross-checked against the NumPy oracle
+ * (tests/test_cpu_port.py), which replays the reference's own recorded run
+ * (tests/test_oracle_testrun.py); the reference itself cannot be built here.
  */
 #include <math.h>
 #include <stddef.h>

@@ -27,12 +27,18 @@ the reference project root).  Numerics:
   give the same Green's functions to rounding because the time-displaced
   Green's function does not depend on the QR convention.
 
-Parity status: parity unpinned.  The reference cannot be compiled here (no
-Fortran compiler, no MPI) and its tests hold no golden vectors for this path,
-so the oracle is not checked against reference outputs.  What pins it instead
-are known-answer tests built from the algorithm itself (ranf closed form,
-free-fermion limit, dense-product Green's function, mu-derivative identity,
-complex/real agreement, lattice invariants); see tests/test_oracle.py.
+Parity status: pinned against the reference's own recorded run.  The
+reference cannot be compiled here (no Fortran compiler, no MPI), but its
+test_run/ directory holds the output of its own binary for one 100-bin run
+(global Wolff moves plus local sweeps, 4x4, Ltrot = 40, absolute = 5).
+Replayed from the same inputs, this oracle reproduces that run's six per-bin
+observable series to 2.3e-14 relative and its acceptance ratios, cluster size
+and drift figures to the printed digits, which requires every accept/reject
+decision to agree (tests/test_oracle_testrun.py, fixture extracted by
+tests/golden/make_testrun_golden.py).  Known-answer tests built from the
+algorithm itself (ranf closed form, free-fermion limit, dense-product
+Green's function, mu-derivative identity, complex/real agreement, lattice
+invariants) cover what that run does not reach; see tests/test_oracle.py.
 """
 from __future__ import annotations
 

@@ -1,7 +1,8 @@
 """Known-answer tests that pin the CPU oracle (oracle/z2_oracle.py).
 
-The reference (Fortran + MPI + LAPACK) cannot be compiled in this image and
-ships no golden vectors, so the oracle is pinned by:
+The reference (Fortran + MPI + LAPACK) cannot be compiled in this image; its
+one recorded run pins the oracle in tests/test_oracle_testrun.py.  Beyond
+that run the oracle is pinned by:
   * the ranf recursion against its closed form,
   * lattice-table invariants (checkerboard groups, plaquettes, translations),
   * the free-fermion limit RT = 0,
