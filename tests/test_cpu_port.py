@@ -9,12 +9,18 @@ from oracle import z2cpu
 import pytest
 
 
-@pytest.mark.parametrize("h", [0.5, 0.0])
-def test_c_port_matches_python_oracle(h):
-    kw = dict(RT=1.0, J=0.5, h=h, mu=0.1, beta=2.0, Nlx=4, Nly=4, Ltrot=20, Nwrap=5)
-    out = z2cpu.run(**kw, seed=2024, nbins=2, record=True)
-    p = zo.Params(RT=1.0, J=0.5, h=h, mu=0.1, Nlx=4, Nly=4, Ltrot=20, beta=2.0, Nwrap=5)
-    c = zo.Z2Chain(p, seed=2024, record_decisions=True)
+@pytest.mark.parametrize("kw, absolute, seed", [
+    (dict(RT=1.0, J=0.5, h=0.5, mu=0.1, beta=2.0, Nlx=4, Nly=4, Ltrot=20, Nwrap=5), 1, 2024),
+    (dict(RT=1.0, J=0.5, h=0.0, mu=0.1, beta=2.0, Nlx=4, Nly=4, Ltrot=20, Nwrap=5), 1, 2024),
+    # the couplings and start of the reference's recorded run (absolute = 5)
+    (dict(RT=0.5, J=1.0, h=0.52, mu=0.3, beta=2.0, Nlx=4, Nly=4, Ltrot=40, Nwrap=5), 5, 12439),
+    # a lattice size of the batched workload
+    (dict(RT=1.0, J=0.5, h=0.6, mu=0.0, beta=2.0, Nlx=6, Nly=6, Ltrot=20, Nwrap=10), 1, 77),
+])
+def test_c_port_matches_python_oracle(kw, absolute, seed):
+    out = z2cpu.run(**kw, seed=seed, nbins=2, absolute=absolute, record=True)
+    p = zo.Params(**kw, absolute=absolute)
+    c = zo.Z2Chain(p, seed=seed, record_decisions=True)
     c.pre()
     obs = []
     for _ in range(2):
