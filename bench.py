@@ -24,35 +24,63 @@ import subprocess
 import sys
 import time
 
+from dataclasses import dataclass
+
 import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 DTAU = 0.1
+WORKLOAD = ("batched: {n} chains per GPU, L in {{6,8,10,12}}, beta in {{8,12,16}}, dtau 0.1, "
+            "h~U[0.2,1], K=J=0.5, t=1, mu=0, Nwrap 10, seeded +-1 links (conf_set absolute=1), "
+            "one bin (sweep_L+sweep_R) of every chain per step")
+
+
+@dataclass
+class ChainSpec:
+    """One chain's parameters (the hot-path lines of paramC_sets.txt and its
+    seed); the fields the library's host binding and the C restatement read."""
+    RT: float
+    J: float
+    h: float
+    mu: float
+    Nlx: int
+    Nly: int
+    Ltrot: int
+    beta: float
+    Nwrap: int
+    absolute: int
+    seed: int
+    Q: float = 1.0
+    rt_bond: object = None
+
+    @property
+    def N(self):
+        return self.Nlx * self.Nly
+
+
 # DRAM bytes (read + write) of one step of the 256-chain workload, from one
 # ncu capture of the chain kernel (dram__bytes_read.sum + dram__bytes_write.sum)
 TRAFFIC_BYTES_PER_STEP = 2995005440 + 5308945664
 
 
 def batched_chains(rank: int = 0, n: int = 256):
-    from z2_gauge_zfy_b200 import Chain
     rng = np.random.default_rng(20240 + rank)
     hs = rng.uniform(0.2, 1.0, n)
     out = []
     for i in range(n):
         L = (6, 8, 10, 12)[i % 4]
         beta = (8.0, 12.0, 16.0)[(i // 4) % 3]
-        out.append(Chain(RT=1.0, J=0.5, h=float(hs[i]), mu=0.0, Nlx=L, Nly=L,
-                         Ltrot=int(round(beta / DTAU)), beta=beta, Nwrap=10, absolute=1,
-                         seed=12345 + rank * 100003 + i))
+        out.append(ChainSpec(RT=1.0, J=0.5, h=float(hs[i]), mu=0.0, Nlx=L, Nly=L,
+                             Ltrot=int(round(beta / DTAU)), beta=beta, Nwrap=10, absolute=1,
+                             seed=12345 + rank * 100003 + i))
     return out
 
 
 def single_chain():
-    from z2_gauge_zfy_b200 import Chain
-    return [Chain(RT=1.0, J=0.5, h=0.5, mu=0.0, Nlx=8, Nly=8, Ltrot=100, beta=10.0, Nwrap=10,
-                  absolute=1, seed=12345)]
+    return [ChainSpec(RT=1.0, J=0.5, h=0.5, mu=0.0, Nlx=8, Nly=8, Ltrot=100, beta=10.0,
+                      Nwrap=10, absolute=1, seed=12345)]
 
 
 def adjoint_cost(device: int) -> dict:
@@ -171,94 +199,181 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def peaks():
-    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    try:
-        with open(path) as f:
-            return json.load(f)
-    except OSError:
-        return {}
+def fp64_peak_tflops(device: int, n: int = 8192, reps: int = 5):
+    """FP64 roofline denominator, measured in this run on this GPU: cuBLAS
+    DGEMM n^3 through torch.matmul on float64 (the FP64 tensor pipe), best of
+    `reps` timed with CUDA events after two warm-up products."""
+    import torch
+    dev = torch.device("cuda", device)
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize(dev)
+    best = float("inf")
+    for _ in range(reps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
 
 
-FP64_PEAK_NOTE = ("measured cuBLAS DGEMM 8192^3 (torch.matmul float64) on this pool, "
-                  "profiles/fp64_peak_b200.md")
+def _cpu_cost(c) -> float:
+    """Relative CPU cost of one bin of a chain for the C restatement: wraps
+    and observables ~ N^2, accepted-flip updates and stabilizations ~ N^3, per
+    slice (acceptance ~0.1 on this workload)."""
+    n = float(c.N)
+    return c.Ltrot * n * n * (92.0 + 0.8 * n + 14.0 * n / c.Nwrap)
 
 
-def fp64_peak_tflops():
-    """FP64 denominator: measured DGEMM throughput committed under profiles/."""
-    path = os.path.join(ROOT, "profiles", "fp64_peak_b200.json")
-    try:
-        with open(path) as f:
-            d = json.load(f)
-        return float(d["dgemm_tflops"]), "measured"
-    except (OSError, KeyError, ValueError):
-        return 40.0, "nominal (B200 datasheet FP64 tensor, not measured)"
-
-
-def _cpu_one(arg):
-    """One chain on one core with the C restatement: pre, then one bin timed."""
-    c, nbins = arg
+def parity_and_cpu_baseline(device: int, kmap: dict) -> tuple[dict, dict]:
+    """The metric's accuracy condition, checked on the benched configuration:
+    one chain of each of the 12 (L, beta) classes of the batched workload plus
+    the single-chain configuration, one bin each in ONE batched launch with
+    the tuned delay ranks, against the C restatement of the reference path
+    (oracle/c/z2cpu.c, reference LAPACK, 1 thread) from the same seeds.  The
+    C restatement's bin times of the 12 batched classes are the 1-core CPU
+    baseline.  Returns (parity, cpu_baseline)."""
     from oracle import z2cpu
-    r = z2cpu.run(RT=c.RT, J=c.J, h=c.h, mu=c.mu, beta=c.beta, Nlx=c.Nlx, Nly=c.Nly,
-                  Ltrot=c.Ltrot, Nwrap=c.Nwrap, seed=c.seed, nbins=nbins, absolute=c.absolute)
-    return 2 * c.N * c.Ltrot * nbins, r["seconds"]
-
-
-def cpu_baseline_sample():
-    """The C restatement of the reference path (reference LAPACK, 1 thread)
-    on a stratified sample of the batched workload: one chain of each of the
-    12 (L, beta) classes, one bin each."""
-    chains = batched_chains()[:12]
+    from z2_gauge_zfy_b200 import Z2Batch
+    chains = batched_chains()[:12] + single_chain()
+    ks = [int(kmap.get(c.N, 0)) for c in chains]
+    with Z2Batch(chains, device=device, record=True, delay_k_chain=ks) as b:
+        b.pre()
+        b.sweep(1, False)
+        gpu = [(b.green(i), b.obs_equal(i), b.stats(i)["Xmaxm"], b.decisions(i)[0],
+                b.get_config(i)) for i in range(len(chains))]
+    g_err = o_err = x_err = 0.0
+    dec_same = cfg_same = True
     su = sec = 0.0
-    for c in chains:
-        a, b = _cpu_one((c, 1))
-        su += a
-        sec += b
-    return {"value": su / sec, "unit": "site-updates/s", "cores": 1, "kind": "port",
+    for i, c in enumerate(chains):
+        cc = z2cpu.CpuChain.from_chain(c)
+        cc.pre()
+        t, obs, dec = cc.bin(record=True)
+        st = cc.state()
+        cc.close()
+        G, og, xg, dg, (sig, iseed) = gpu[i]
+        g_err = max(g_err, float(np.max(np.abs(G - st["G"])) / np.max(np.abs(st["G"]))))
+        ov = np.array(list(og.values()))
+        o_err = max(o_err, float(np.max(np.abs(ov - obs) / np.maximum(np.abs(obs), 1.0))))
+        x_err = max(x_err, abs(xg - st["Xmaxm"]) / max(st["Xmaxm"], 1e-12))
+        dec_same = dec_same and bool(np.array_equal(dg, dec))
+        cfg_same = cfg_same and bool(np.array_equal(sig, st["sigma"])) and iseed == st["iseed"]
+        if i < 12:
+            su += 2 * c.N * c.Ltrot
+            sec += t
+    parity = {"max_g_rel_err": g_err, "g_err_bound": 1e-8, "g_err_ok": g_err <= 1e-8,
+              "decisions_identical": dec_same, "links_and_ranf_identical": cfg_same,
+              "max_obs_rel_err": o_err, "max_xmaxm_rel_err": x_err,
+              "sample": "one bin of one chain of each of the 12 (L, beta) classes + the "
+                        "single-chain configuration (L=8, beta=10), one batched launch with the "
+                        "tuned delay ranks, against the C restatement from the same seeds"}
+    base = {"value": su / sec, "unit": "site-updates/s", "cores": 1, "kind": "port",
             "sample": "C restatement (oracle/c/z2cpu.c, reference LAPACK via OpenBLAS, 1 thread, "
                       "one spin sector, real arithmetic: a lower bound on the reference's cost), "
                       "one bin of one chain of each of the 12 (L, beta) classes"}
+    return parity, base
+
+
+def _ref_worker(conn, chains):
+    """One host core of the reference arm: owns its chains for the whole run
+    (the reference keeps a chain in its process between bins), runs Local_sweep
+    pre once, then one bin of every owned chain per 'bin' message."""
+    from oracle import z2cpu
+    cs = [z2cpu.CpuChain.from_chain(c) for c in chains]
+    for c in cs:
+        c.pre()
+    conn.send("ready")
+    while conn.recv() == "bin":
+        for c in cs:
+            c.bin()
+        conn.send("done")
+    for c in cs:
+        c.close()
 
 
 def run_reference(args):
-    """Reference arm: the C restatement of the reference path on all host
-    cores, one chain per process (the reference runs one chain per MPI rank)."""
+    """Reference arm: the C restatement of the reference path (the reference
+    cannot be built in this image: Fortran + MPI) on every host core, on the
+    SAME workload as the GPU arm: the 256 chains of the batched workload, each
+    step one bin of every chain, timed by wall clock.  Chains are placed on the
+    cores longest-first (greedy by estimated cost) and stay there, as the
+    reference runs each chain in its own MPI rank (src/main.f90:23-25)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     import multiprocessing as mp
     from oracle import build_cpu
     build_cpu.build()
-    cores = os.cpu_count() or 1
-    chains = batched_chains()
+    try:
+        cores = len(os.sched_getaffinity(0))
+    except AttributeError:
+        cores = os.cpu_count() or 1
+    chains = batched_chains(0, args.chains)
+    load = [0.0] * cores
+    parts = [[] for _ in range(cores)]
+    for c in sorted(chains, key=_cpu_cost, reverse=True):
+        w = min(range(cores), key=lambda j: load[j])
+        parts[w].append(c)
+        load[w] += _cpu_cost(c)
     ctx = mp.get_context("spawn")
-    with ctx.Pool(cores) as pool:
-        for w in range(args.warmup):
-            pool.map(_cpu_one, [(c, 1) for c in chains[:cores]])
-        su_tot = t_tot = 0.0
-        for step in range(args.steps):
-            # each step: one bin of `cores` chains in parallel; the step's time
-            # is the slowest process (all start together)
-            sample = [chains[(step * cores + i) % len(chains)] for i in range(cores)]
-            res = pool.map(_cpu_one, [(c, 1) for c in sample])
-            su_tot += sum(r[0] for r in res)
-            t_tot += max(r[1] for r in res)
-    v = su_tot / t_tot
+    conns, procs = [], []
+    for part in parts:
+        a, b = ctx.Pipe()
+        pr = ctx.Process(target=_ref_worker, args=(b, part), daemon=True)
+        pr.start()
+        conns.append(a)
+        procs.append(pr)
+    for a in conns:
+        if a.recv() != "ready":
+            raise RuntimeError("reference worker failed to start")
+
+    def step():
+        t0 = time.perf_counter()
+        for a in conns:
+            a.send("bin")
+        for a in conns:
+            if a.recv() != "done":
+                raise RuntimeError("reference worker failed")
+        return time.perf_counter() - t0
+
+    for _ in range(args.warmup):
+        step()
+    t_tot = sum(step() for _ in range(args.steps))
+    for a in conns:
+        a.send("stop")
+    for pr in procs:
+        pr.join(timeout=30)
+    su_step = site_updates(chains)
+    v = su_step * args.steps / t_tot
     line = {"impl": "reference", "metric": "spacetime site-updates/s", "value": v,
             "unit": "site-updates/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_tot * 1e3 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded +-1 links, conf_set absolute=1)",
-            "config": {"workload": "batched: chains L in {6,8,10,12}, beta in {8,12,16}, dtau 0.1, "
-                                   "h~U[0.2,1], K=0.5, Nwrap 10, one bin per chain; reference arm "
-                                   f"runs {cores} chains per step, one per host core"},
+            "config": workload_config(chains),
             "cpu_baseline": {"value": v, "unit": "site-updates/s", "cores": cores, "kind": "port",
-                             "sample": f"{cores} chains x 1 bin per step, one chain per process, "
-                                       "C restatement with reference LAPACK (1 BLAS thread each)"},
+                             "sample": f"the whole workload every step: {len(chains)} chains x 1 "
+                                       f"bin on {cores} processes (one per host core, chains "
+                                       "resident, placed longest-first), wall clock; C "
+                                       "restatement with reference LAPACK, 1 BLAS thread each"},
             "e2e": {"value": v, "unit": "site-updates/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def workload_config(chains) -> dict:
+    """The `config` of both arms' lines: the workload only."""
+    return {"workload": WORKLOAD.format(n=len(chains)), "chains_per_gpu": len(chains),
+            "site_updates_per_step_per_gpu": site_updates(chains),
+            "l2": "inputs larger than L2 (per-GPU chain state > 126 MB)"}
 
 
 def main():
@@ -338,28 +453,35 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dev_s, e2e_s = float(t[0]), float(t[1])
 
+    # bin observables of every chain of every rank, averaged as the reference
+    # averages them over its MPI ranks (one all-reduce after the timed region)
+    from z2_gauge_zfy_b200.replicas import reduce_bin_observables
+    obs_local = np.array([list(b.obs_equal(i).values()) for i in range(len(chains))])
+    obs_mean = reduce_bin_observables(obs_local, device=f"cuda:{local}" if dist else "cpu")
+
     total_su = su_step * args.steps * world
     value = total_su / dev_s
     e2e = total_su / e2e_s
     flops_launch = algorithmic_flops(chains, a_rate)
     launch_s = dev_s / args.steps
-    peak, peak_kind = fp64_peak_tflops()
+    b.close()
+    peak = fp64_peak_tflops(local)
     achieved = flops_launch / launch_s / 1e12
+    kmap = {c.N: int(k) for c, k in zip(chains, kchain)}
     line = {
         "metric": "spacetime site-updates/s", "value": value, "unit": "site-updates/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": dev_s * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded +-1 links, conf_set absolute=1)",
-        "config": {"workload": "batched: 256 chains per GPU, L in {6,8,10,12}, beta in "
-                               "{8,12,16}, dtau 0.1, h~U[0.2,1], K=J=0.5, t=1, mu=0, Nwrap 10, "
-                               "one bin (sweep_L+sweep_R) per step",
-                   "chains_per_gpu": len(chains), "site_updates_per_step_per_gpu": su_step,
-                   "parallelism": f"chains sharded over {world} GPU(s), replicas",
-                   "l2": "inputs larger than L2 (per-GPU chain state > 126 MB)",
-                   "accept_rate": a_rate,
-                   "delay_rank": {str(c.N): int(k) for c, k in zip(chains, kchain)},
-                   "autotune_s": t_tune},
+        "config": workload_config(chains),
+        "parallelism": f"chains sharded over {world} GPU(s), replicas",
+        "accept_rate": a_rate,
+        "delay_rank": ",".join(f"N{n}:k{k}" for n, k in sorted(kmap.items())),
+        "autotune_s": t_tune,
+        "bin_observables_mean": dict(zip(("flux_avg", "chi_flux", "pair_sc_q0", "cdw_pi",
+                                          "cdw_shift", "cdw_ratio", "density"),
+                                         obs_mean.tolist())),
         "e2e": {"value": e2e, "unit": "site-updates/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": len(chains) * 7 * 8},
         "gpu_launches": args.steps,
@@ -369,9 +491,9 @@ def main():
                      "traffic": TRAFFIC_BYTES_PER_STEP if len(chains) == 256 else None,
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
                                        "bench step (256 chains)",
-                     "note": f"FP64 algorithmic flops per launch / launch time; peak {peak_kind}"},
+                     "note": "FP64 algorithmic flops per launch / launch time; peak = cuBLAS "
+                             "DGEMM 8192^3 (torch.matmul float64) measured in this run"},
     }
-    b.close()
     if rank == 0 and not args.no_single:
         sb = Z2Batch(single_chain(), device=local)
         sb.pre()
@@ -387,8 +509,11 @@ def main():
     if rank == 0 and not args.no_single:
         line["adjoint"] = adjoint_cost(local)
         line["large_batched"] = large_batched(local)
-    if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_sample()
+    if rank == 0:
+        parity, base = parity_and_cpu_baseline(local, kmap)
+        line["parity"] = parity
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = base
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

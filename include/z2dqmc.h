@@ -212,8 +212,10 @@ int z2_stab_green_big(z2_handle *h, int32_t chain, const double *UR,
  * rejected with Z2_ERR_ARG.  The work is enqueued on `stream` (a
  * cudaStream_t, NULL = default stream); the call returns after the launch.
  * The first call on a device looks up the device address of the scratch
- * array (cudaGetSymbolAddress) with that device current; make that first
- * call before any stream capture.  Every call shares the one scratch array,
+ * array (cudaGetSymbolAddress) with that device current, and so does the
+ * first call after the device's context changes (e.g. after
+ * cudaDeviceReset); make such a call before any stream capture.  Every call
+ * shares the one scratch array,
  * so calls that overlap on the GPU (other streams, other host threads) race;
  * no part of the scratch needs to start at zero. ---- */
 #define Z2_NOALLOC_NMAX 144

@@ -26,10 +26,13 @@ def build(force: bool = False) -> str:
     if not force and os.path.exists(OUT) and os.path.getmtime(OUT) >= os.path.getmtime(SRC):
         return OUT
     libdir, lib = openblas()
-    cmd = ["gcc", "-O2", "-std=gnu11", "-fPIC", "-shared", SRC, "-o", OUT + ".tmp",
+    # a per-process temporary name: ranks started together on a fresh
+    # checkout build side by side and the last os.replace wins
+    tmp = f"{OUT}.tmp.{os.getpid()}"
+    cmd = ["gcc", "-O2", "-std=gnu11", "-fPIC", "-shared", SRC, "-o", tmp,
            "-L" + libdir, "-l:" + lib, "-Wl,-rpath," + libdir, "-lm"]
     subprocess.run(cmd, check=True)
-    os.replace(OUT + ".tmp", OUT)
+    os.replace(tmp, OUT)
     return OUT
 
 

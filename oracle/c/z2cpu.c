@@ -66,7 +66,7 @@ typedef struct {
   double *tau, *Dn;
   /* accumulators */
   double flux_sum, flux_sq, pair, cdw, cdws, dens, nobs;
-  double acc_num, acc_den, Xmaxm, Xmeanm;
+  double acc_num, acc_den, Xmaxm, Xmeanm, acc_sum;
   unsigned char *dec;   /* optional [2][Ltrot][nb] */
 } Chain;
 
@@ -515,24 +515,29 @@ static double now(void) {
 }
 
 /*
- * One chain: seeded start (conf_set absolute = 1..5 on the run lattice),
- * Local_sweep_pre, then nbins bins of nsweep (sweep_L, sweep_R) pairs.
- * dparams = {RT, J, h, mu, beta}; iparams = {Nlx, Nly, Ltrot, Nwrap,
- * absolute, seed, nbins, nsweep}.  Outputs: obs [nbins][7] (flux_avg,
- * chi_flux, pair_sc_q0, cdw_pi, cdw_shift, cdw_ratio, density), the final G
- * (column-major), the decisions of the last half-sweeps [2][Ltrot][2N]
- * (optional), stats {acc, Xmaxm, Xmeanm, iseed}, and the seconds spent in the
- * bins (pre excluded).  Returns 0.
+ * Persistent chains (the reference keeps one chain's state in its process
+ * between bins, src/main.f90:70-110):
+ *   z2cpu_new   seeded start, conf_set absolute = 1 / 3 / 5 on the run
+ *               lattice (src/fields.f90:311-427) + the lambda_random_fill
+ *               draws; dparams = {RT, J, h, mu, beta}, iparams = {Nlx, Nly,
+ *               Ltrot, Nwrap, absolute, seed}.
+ *   z2cpu_pre   Local_sweep_pre (src/local_sweep.f90:87-104).
+ *   z2cpu_bin   one bin of nsweep (sweep_L, sweep_R) pairs
+ *               (src/local_sweep.f90:152-195); obs[7] = flux_avg, chi_flux,
+ *               pair_sc_q0, cdw_pi, cdw_shift, cdw_ratio, density; dec
+ *               (optional) receives the decisions of the last half-sweeps
+ *               [2][Ltrot][2N]; returns the seconds spent.
+ *   z2cpu_state G (column-major), sigma [Ltrot][2N] as +-1 doubles, stats
+ *               {acc (sum over bins), Xmaxm, Xmeanm, iseed}; each optional.
+ *   z2cpu_free  releases the chain.
  */
-int z2cpu_run(const double *dparams, const int *iparams, double *obs, double *Gout,
-              unsigned char *dec, double *stats, double *seconds) {
+void *z2cpu_new(const double *dparams, const int *iparams) {
   scipy_openblas_set_num_threads(1);
-  Chain C;
-  memset(&C, 0, sizeof(C));
-  Chain *c = &C;
+  Chain *c = calloc(1, sizeof(Chain));
+  if (!c) return NULL;
   c->RT = dparams[0]; c->J = dparams[1]; c->h = dparams[2]; c->mu = dparams[3]; c->beta = dparams[4];
   c->Lx = iparams[0]; c->Ly = iparams[1]; c->Ltrot = iparams[2]; c->Nwrap = iparams[3];
-  int absolute = iparams[4], seed = iparams[5], nbins = iparams[6], nsweep = iparams[7];
+  int absolute = iparams[4], seed = iparams[5];
   c->N = c->Lx * c->Ly; c->nb = 2 * c->N; c->Nst = c->Ltrot / c->Nwrap;
   c->dtau = c->beta / (double)c->Ltrot;
   c->alpha = 0.5 * c->dtau * c->RT; c->alpha2 = c->dtau * c->RT;
@@ -564,30 +569,76 @@ int z2cpu_run(const double *dparams, const int *iparams, double *obs, double *Go
   c->jpvt = malloc(sizeof(int) * N);
   c->lwork = 64 * N + 64;
   c->work = malloc(sizeof(double) * c->lwork);
+  c->acc_sum = 0.0;
+  return c;
+}
+
+void z2cpu_pre(void *h) {
+  scipy_openblas_set_num_threads(1);
+  pre((Chain *)h);
+}
+
+double z2cpu_bin(void *h, int nsweep, double *obs, unsigned char *dec) {
+  scipy_openblas_set_num_threads(1);
+  Chain *c = (Chain *)h;
+  const int N = c->N;
   c->dec = dec;
-  pre(c);
   double t0 = now();
-  double acc_sum = 0.0;
-  for (int b = 0; b < nbins; ++b) {
-    c->flux_sum = c->flux_sq = c->pair = c->cdw = c->cdws = c->dens = c->nobs = 0.0;
-    c->acc_num = c->acc_den = 0.0;
-    reset_h0(c);
-    for (int s = 0; s < nsweep; ++s) { sweep_L(c); sweep_R(c); }
-    double z = 1.0 / c->nobs, fm = c->flux_sum * z, fsq = c->flux_sq * z;
-    double *o = obs + 7 * b;
-    o[0] = fm;
-    o[1] = c->beta * (double)N * fmax(0.0, fsq - fm * fm);
-    o[2] = (c->pair * z) / (double)N;
-    o[3] = (c->cdw * z) / (double)N;
-    o[4] = (c->cdws * z) / (double)N;
-    o[5] = (o[3] > 1.0e-12) ? 1.0 - o[4] / o[3] : 0.0;
-    o[6] = c->dens * z;
-    if (c->acc_den > 0.0) acc_sum += c->acc_num / c->acc_den;
+  c->flux_sum = c->flux_sq = c->pair = c->cdw = c->cdws = c->dens = c->nobs = 0.0;
+  c->acc_num = c->acc_den = 0.0;
+  reset_h0(c);
+  for (int s = 0; s < nsweep; ++s) { sweep_L(c); sweep_R(c); }
+  double z = 1.0 / c->nobs, fm = c->flux_sum * z, fsq = c->flux_sq * z;
+  double o[7];
+  o[0] = fm;
+  o[1] = c->beta * (double)N * fmax(0.0, fsq - fm * fm);
+  o[2] = (c->pair * z) / (double)N;
+  o[3] = (c->cdw * z) / (double)N;
+  o[4] = (c->cdws * z) / (double)N;
+  o[5] = (o[3] > 1.0e-12) ? 1.0 - o[4] / o[3] : 0.0;
+  o[6] = c->dens * z;
+  if (c->acc_den > 0.0) c->acc_sum += c->acc_num / c->acc_den;
+  double sec = now() - t0;
+  if (obs) memcpy(obs, o, sizeof(o));
+  c->dec = NULL;
+  return sec;
+}
+
+void z2cpu_state(void *h, double *Gout, double *sigma, double *stats) {
+  Chain *c = (Chain *)h;
+  if (Gout) memcpy(Gout, c->G, sizeof(double) * c->N * c->N);
+  if (sigma) memcpy(sigma, c->sigma, sizeof(double) * c->nb * c->Ltrot);
+  if (stats) {
+    stats[0] = c->acc_sum; stats[1] = c->Xmaxm; stats[2] = c->Xmeanm; stats[3] = (double)c->iq;
   }
-  *seconds = now() - t0;
-  if (Gout) memcpy(Gout, c->G, sizeof(double) * NN);
-  stats[0] = acc_sum; stats[1] = c->Xmaxm; stats[2] = c->Xmeanm; stats[3] = (double)c->iq;
-  free(m); free(c->DR); free(c->URs); free(c->DRs); free(c->jpvt); free(c->work);
+}
+
+void z2cpu_free(void *h) {
+  Chain *c = (Chain *)h;
+  if (!c) return;
+  free(c->G); free(c->DR); free(c->URs); free(c->DRs); free(c->jpvt); free(c->work);
   free(c->sigma); free(c->bond); free(c->grp); free(c->bb); free(c->xy); free(c->plaq);
+  free(c);
+}
+
+/*
+ * One chain from a seeded start to nbins bins (z2cpu_new, z2cpu_pre, then
+ * z2cpu_bin per bin).  iparams = {Nlx, Nly, Ltrot, Nwrap, absolute, seed,
+ * nbins, nsweep}.  Outputs: obs [nbins][7], the final G (column-major), the
+ * decisions of the last half-sweeps [2][Ltrot][2N] (optional), stats {acc,
+ * Xmaxm, Xmeanm, iseed}, and the seconds spent in the bins (pre excluded).
+ * Returns 0, or 1 when the chain cannot be allocated.
+ */
+int z2cpu_run(const double *dparams, const int *iparams, double *obs, double *Gout,
+              unsigned char *dec, double *stats, double *seconds) {
+  void *c = z2cpu_new(dparams, iparams);
+  if (!c) return 1;
+  const int nbins = iparams[6], nsweep = iparams[7];
+  z2cpu_pre(c);
+  double sec = 0.0;
+  for (int b = 0; b < nbins; ++b) sec += z2cpu_bin(c, nsweep, obs + 7 * b, dec);
+  *seconds = sec;
+  z2cpu_state(c, Gout, NULL, stats);
+  z2cpu_free(c);
   return 0;
 }

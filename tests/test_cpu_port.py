@@ -36,3 +36,25 @@ def test_c_port_matches_python_oracle(kw, absolute, seed):
     assert out["iseed"] == c.rng.state
     assert np.max(np.abs(out["G"] - c.prop.Gr)) < 1e-12
     assert np.allclose(out["obs"], np.array(obs), rtol=1e-12, atol=1e-13)
+
+
+def test_persistent_chain_matches_run_and_oracle_sigma():
+    """CpuChain (z2cpu_new / pre / bin / state) gives the same bins as
+    z2cpu.run, and its links and ranf state after two bins equal the
+    oracle's."""
+    kw = dict(RT=1.0, J=0.5, h=0.6, mu=0.1, beta=2.0, Nlx=6, Nly=6, Ltrot=20, Nwrap=10)
+    out = z2cpu.run(**kw, seed=91, nbins=2, record=True)
+    c = z2cpu.CpuChain(**kw, seed=91)
+    c.pre()
+    obs = [c.bin(record=True) for _ in range(2)]
+    st = c.state()
+    c.close()
+    assert np.array_equal(obs[-1][2], out["decisions"])
+    assert np.array_equal(np.stack([o[1] for o in obs]), out["obs"])
+    assert np.array_equal(st["G"], out["G"]) and st["iseed"] == out["iseed"]
+    p = zo.Params(**kw)
+    o = zo.Z2Chain(p, seed=91)
+    o.pre()
+    o.sweep()
+    o.sweep()
+    assert np.array_equal(st["sigma"], o.sigma) and st["iseed"] == o.rng.state

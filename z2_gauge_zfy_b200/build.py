@@ -50,21 +50,25 @@ def build_driver(force: bool = False) -> str:
             and os.path.getmtime(DRIVER) >= max(os.path.getmtime(DRIVER_SRC),
                                                 os.path.getmtime(OUT))):
         return DRIVER
+    tmp = f"{DRIVER}.tmp.{os.getpid()}"
     cmd = ["g++", "-O2", "-std=c++17", DRIVER_SRC, "-L" + HERE, "-lz2dqmc",
-           "-Wl,-rpath,$ORIGIN", "-o", DRIVER + ".tmp"]
+           "-Wl,-rpath,$ORIGIN", "-o", tmp]
     subprocess.run(cmd, check=True)
-    os.replace(DRIVER + ".tmp", DRIVER)
+    os.replace(tmp, DRIVER)
     return DRIVER
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
     if force or not up_to_date():
-        cmd = [nvcc(), *NVCC_FLAGS, "-o", OUT + ".tmp", SRC]
+        # per-process temporary name: ranks that start together on a fresh
+        # checkout may build side by side; os.replace makes the swap atomic
+        tmp = f"{OUT}.tmp.{os.getpid()}"
+        cmd = [nvcc(), *NVCC_FLAGS, "-o", tmp, SRC]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-        os.replace(OUT + ".tmp", OUT)
+        os.replace(tmp, OUT)
     build_driver(force)
     return OUT
 

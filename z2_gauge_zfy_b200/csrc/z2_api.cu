@@ -1238,6 +1238,8 @@ extern "C" int z2_stab_green_big(z2_handle *h, int32_t chain, const double *UR, 
 // the file-scope array below, which every GPU that loads this library keeps
 // until the process exits: 5 * Z2_NOALLOC_NMAX^2 doubles (829,440 bytes).
 // ---------------------------------------------------------------------------
+#include <cuda.h>   // CUcontext / CUresult types of the two driver entry points below
+
 #include <mutex>
 
 static __device__ __align__(256) double z2_noalloc_scratch[5 * Z2_NOALLOC_NMAX * Z2_NOALLOC_NMAX];
@@ -1279,6 +1281,34 @@ static constexpr size_t noalloc_smem_bytes(int N) {
 // within the 48 KB a launch gets without opting in to more
 static_assert(noalloc_smem_bytes(Z2_NOALLOC_NMAX) <= 48 * 1024, "no-alloc shared memory");
 
+// Identity of the calling thread's current CUDA context: a 64-bit id that the
+// driver never reuses within a process (cuCtxGetId), or 0 when no context is
+// current or the driver does not offer the call.  The driver entry points
+// come through the runtime, so the library needs no link to libcuda.
+static unsigned long long current_ctx_id() {
+  typedef CUresult (*get_current_t)(CUcontext *);
+  typedef CUresult (*get_id_t)(CUcontext, unsigned long long *);
+  static get_current_t get_current = nullptr;
+  static get_id_t get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = (get_current_t)f;
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = (get_id_t)f;
+  });
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+  if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
 extern "C" int z2_stab_green_noalloc(int32_t N, int32_t nt, int32_t Ltrot, const double *UR,
                                      const double *DR, const double *VR, const double *UL,
                                      const double *DL, const double *VL, double *G,
@@ -1289,18 +1319,26 @@ extern "C" int z2_stab_green_noalloc(int32_t N, int32_t nt, int32_t Ltrot, const
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return Z2_ERR_CUDA;
   // Set-up, once per device with that device current: the device address of
-  // the scratch array (host code must not use the symbol itself).
+  // the scratch array (host code must not use the symbol itself).  The
+  // address belongs to the context the array was loaded into, so it is looked
+  // up again when the device's current context changes (a new context after
+  // cudaDeviceReset, or a caller's own driver-API context).
+  struct Slot { unsigned long long ctx; double *ptr; };
   static std::mutex mu;
-  static double *scratch_of[64] = {nullptr};
+  static Slot scratch_of[64] = {};
   double *scratch = nullptr;
   {
     std::lock_guard<std::mutex> lock(mu);
-    if (!scratch_of[dev]) {
+    const unsigned long long id = current_ctx_id();
+    Slot &sl = scratch_of[dev];
+    if (!sl.ptr || id == 0 || sl.ctx != id) {
       void *p = nullptr;
       if (cudaGetSymbolAddress(&p, z2_noalloc_scratch) != cudaSuccess || !p) return Z2_ERR_CUDA;
-      scratch_of[dev] = (double *)p;
+      sl.ptr = (double *)p;
+      // the lookup makes the runtime's context current when none was
+      sl.ctx = id ? id : current_ctx_id();
     }
-    scratch = scratch_of[dev];
+    scratch = sl.ptr;
   }
   z2_stab_green_noalloc_kernel<<<1, Z2_NT, noalloc_smem_bytes(N), (cudaStream_t)stream>>>(
       N, nt, Ltrot, UR, DR, VR, UL, DL, VL, G, scratch);
