@@ -400,9 +400,15 @@ def main():
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
 
-    import __graft_entry__
-    __graft_entry__.build()
-    from z2_gauge_zfy_b200 import Z2Batch, tune_delay
+    # one build per node: local rank 0 compiles (if the tree is stale), the
+    # other ranks wait at a barrier and then load the built library
+    if local == 0:
+        import __graft_entry__
+        __graft_entry__.build()
+    if dist is not None:
+        dist.barrier()
+    from z2_gauge_zfy_b200 import Z2Batch, load, tune_delay
+    load()
 
     chains = batched_chains(rank, args.chains)
     su_step = site_updates(chains)
@@ -455,8 +461,8 @@ def main():
 
     # bin observables of every chain of every rank, averaged as the reference
     # averages them over its MPI ranks (one all-reduce after the timed region)
-    from z2_gauge_zfy_b200.replicas import reduce_bin_observables
-    obs_local = np.array([list(b.obs_equal(i).values()) for i in range(len(chains))])
+    from z2_gauge_zfy_b200.replicas import bin_observables, reduce_bin_observables
+    obs_local = bin_observables(b)
     obs_mean = reduce_bin_observables(obs_local, device=f"cuda:{local}" if dist else "cpu")
 
     total_su = su_step * args.steps * world

@@ -1,6 +1,8 @@
 """Replica plumbing on CPU: two gloo ranks each run their own oracle chains
-(distinct seeds), reduce the bin observables and the timing exactly as the
-GPU ranks do with NCCL."""
+(distinct seeds), read the bin observables back through the product's
+readback path (Z2Batch.obs_equal over a stand-in library that serves the
+oracle's values, as bench.py reads its batch) and reduce them and the timing
+exactly as the GPU ranks do with NCCL."""
 import os
 import socket
 
@@ -15,6 +17,19 @@ def _free_port():
         return s.getsockname()[1]
 
 
+class _ObsLib:
+    """Stand-in library: z2_get_obs_equal writes the given rows into the
+    caller's buffer, as the CUDA library copies a chain's bin observables."""
+
+    def __init__(self, rows):
+        self.rows = rows
+
+    def z2_get_obs_equal(self, h, chain, buf):
+        for q, v in enumerate(self.rows[chain]):
+            buf[q] = v
+        return 0
+
+
 def _worker(rank, world, port, out):
     import torch.distributed as dist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
@@ -22,7 +37,9 @@ def _worker(rank, world, port, out):
     from datetime import timedelta
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
     from oracle import z2_oracle as zo
-    from z2_gauge_zfy_b200.replicas import chain_seed, max_over_ranks, reduce_bin_observables
+    from z2_gauge_zfy_b200 import api
+    from z2_gauge_zfy_b200.replicas import (bin_observables, chain_seed, max_over_ranks,
+                                            reduce_bin_observables)
     p = zo.Params(RT=1.0, J=0.5, h=0.5, mu=0.0, Nlx=4, Nly=4, Ltrot=10, beta=1.0, Nwrap=5)
     rows = []
     for i in range(2):
@@ -30,8 +47,10 @@ def _worker(rank, world, port, out):
         c.pre()
         c.sweep()
         d = c.obs.as_dict()
-        rows.append([d[k] for k in ("flux_avg", "chi_flux", "pair_sc_q0", "cdw_pi", "density")])
-    mean = reduce_bin_observables(np.array(rows))
+        rows.append([d[k] for k in api.OBS_EQ_NAMES])
+    b = api.Z2Batch.__new__(api.Z2Batch)       # no z2_create: nothing on a device
+    b.lib, b.h, b.chains = _ObsLib(rows), None, [None, None]
+    mean = reduce_bin_observables(bin_observables(b))
     tmax = max_over_ranks(1.0 + rank)
     out[rank] = (np.array(rows), mean, tmax)
     dist.barrier()

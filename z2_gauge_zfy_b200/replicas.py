@@ -19,6 +19,14 @@ def chain_seed(base: int, rank: int, index: int) -> int:
     return base + rank * 100003 + index
 
 
+def bin_observables(batch) -> np.ndarray:
+    """The bin observables of every chain of a ``Z2Batch`` as an array
+    [n_chains, 7] in the order of ``OBS_EQ_NAMES`` (``z2_get_obs_equal``,
+    the fields Obs_equal_ave writes, src/obser_equal.f90:50-71)."""
+    return np.array([list(batch.obs_equal(i).values()) for i in range(len(batch.chains))],
+                    dtype=np.float64)
+
+
 def reduce_bin_observables(obs: np.ndarray, group=None, device: str = "cpu") -> np.ndarray:
     """Mean over every chain of every rank.  `obs` is [n_local_chains, n_obs]."""
     import torch
