@@ -200,6 +200,62 @@ int z2_stab_green_big(z2_handle *h, int32_t chain, const double *UR,
                       const double *DL, const double *VL, double *G00,
                       double *G0t, double *Gt0, double *Gtt);
 
+/* ---- module-level mirrors on a chain's resident state ----
+ * Each call runs one procedure of the reference's modules on one chain of the
+ * handle, on the state the handle keeps on the device between calls, so that
+ * a driver can replace the modules one at a time:
+ *   Propagator   G, UR DR VR, UL DL VL (src/process_matrix.f90:7-12)
+ *   WrapList     the UDV stacks of both chains (src/process_matrix.f90:26-31)
+ *   Dyn copy     the propagator copy and PropGreen G00, G0t, Gt0, Gtt of the
+ *                time-displaced chain (src/dynamics.f90:8-12)
+ *   sigma, the ranf state, the observable sums of the bin.
+ * nt is a slice 1..Ltrot for per-slice procedures and a stabilization point
+ * (a multiple of Nwrap, 0..Ltrot) for the wraps; anything else is Z2_ERR_ARG.
+ * The Fortran module procedures take both spin sectors (PropU, PropD); the
+ * sectors are identical, so one call covers both.
+ * multiply (src/multiply.f90:8-130): */
+int z2_propK_pre(z2_handle *h, int32_t chain, int32_t nt);  /* UR <- B_nt UR (RT > Zero)    */
+int z2_propK_L(z2_handle *h, int32_t chain, int32_t nt);    /* G <- B^-1 G B, UL <- UL B    */
+int z2_propK_R(z2_handle *h, int32_t chain, int32_t nt);    /* G <- B G B^-1, UR <- B UR    */
+int z2_propgrK_R(z2_handle *h, int32_t chain, int32_t nt);  /* Gt0 <- B Gt0, G0t <- G0t B^-1,
+                                                               Gtt <- B Gtt B^-1, Dyn UR <- B UR */
+int z2_propT_pre(z2_handle *h, int32_t chain);  /* UR *= e^{dtau mu}                          */
+int z2_propT_L(z2_handle *h, int32_t chain);    /* G *= e^{dtau mu} e^{-dtau mu}, UL *= e^{..} */
+int z2_propT_R(z2_handle *h, int32_t chain);    /* G likewise, UR *= e^{dtau mu}              */
+int z2_propgrT_R(z2_handle *h, int32_t chain);  /* the mu factors of propgrT_R               */
+/* stabilization (src/stabilization.f90:374-514); flag = Xmeanm is accumulated
+ * (the reference's `flag` argument of Wrap_L / Wrap_R). */
+int z2_wrap_pre(z2_handle *h, int32_t chain, int32_t nt);
+int z2_wrap_L(z2_handle *h, int32_t chain, int32_t nt, int32_t flag);
+int z2_wrap_R(z2_handle *h, int32_t chain, int32_t nt, int32_t flag);
+int z2_wrap_tau(z2_handle *h, int32_t chain, int32_t nt);    /* nt >= Nwrap, on the Dyn copy */
+/* dynamics: Dyn_reset (src/dynamics.f90:41-48) */
+int z2_dyn_reset(z2_handle *h, int32_t chain);
+/* localK: LocalK_prop_L / LocalK_prop_R (src/localK.f90:347-398), the slice's
+ * 2N flip proposals with its propagation (decisions recorded as by z2_sweep
+ * when the handle records them). */
+int z2_prop_slice_L(z2_handle *h, int32_t chain, int32_t nt);
+int z2_prop_slice_R(z2_handle *h, int32_t chain, int32_t nt);
+/* local_sweep: Local_sweep_reset (src/local_sweep.f90:56-71) */
+int z2_sweep_reset(z2_handle *h, int32_t chain, int32_t toggle);
+/* obser_equal / obser_tau: calc adds slice nt to the bin's sums
+ * (src/obser_equal.f90:73-149, src/obser_tau.f90:56-133); ave divides them by
+ * the count (src/obser_equal.f90:50-71, src/obser_tau.f90:37-47) into what
+ * z2_get_obs_equal / z2_get_obs_tau read. */
+int z2_obs_equal_calc(z2_handle *h, int32_t chain, int32_t nt);
+int z2_obs_equal_ave(z2_handle *h, int32_t chain, int32_t nobs);
+int z2_obs_tau_calc(z2_handle *h, int32_t chain, int32_t nt);
+int z2_obs_tau_ave(z2_handle *h, int32_t chain, int32_t nobst);
+/* State transfer: the Propagator (each buffer optional; N x N column-major,
+ * D vectors of length N) and the PropGreen of the Dyn copy. */
+int z2_get_prop(const z2_handle *h, int32_t chain, double *G, double *UR, double *DR,
+                double *VR, double *UL, double *DL, double *VL);
+int z2_set_prop(z2_handle *h, int32_t chain, const double *G, const double *UR,
+                const double *DR, const double *VR, const double *UL, const double *DL,
+                const double *VL);
+int z2_get_propgr(const z2_handle *h, int32_t chain, double *G00, double *G0t, double *Gt0,
+                  double *Gtt);
+
 /* ---- allocation-free stab_green.  No counterpart in the reference.
  * For callers that cannot call cudaMalloc (their device memory is owned by
  * another allocator, e.g. a framework's caching allocator or a driver that

@@ -93,9 +93,9 @@ def _header_arity():
 
 
 def test_fortran_binding_matches_header():
-    """INTEGRATION.md's ISO_C_BINDING module binds every entry point of the
+    """include/z2_cuda_mod.f90's ISO_C_BINDING module binds every entry point of the
     header, each with the header's number of arguments."""
-    txt = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    txt = open(os.path.join(ROOT, "include", "z2_cuda_mod.f90")).read()
     txt = re.sub(r"&\s*\n\s*", " ", txt)           # join continuation lines
     fort = {}
     for m in re.finditer(r"function\s+(z2_[a-z0-9_]+)\s*\(([^)]*)\)\s*bind\(C,\s*name=\"(\w+)\"\)",
@@ -115,3 +115,24 @@ def test_ctypes_signatures_match_header():
     lib = _ffi.load()
     for name, n in _header_arity().items():
         assert len(getattr(lib, name).argtypes) == n, name
+
+
+def test_fortran_module_is_well_formed():
+    """No Fortran compiler is available here, so the module's structure is
+    checked by reading it: free-form lines of at most 132 characters, every
+    interface function closed, one interface block, module opened and closed."""
+    src = open(os.path.join(ROOT, "include", "z2_cuda_mod.f90")).read()
+    lines = src.splitlines()
+    assert all(len(ln) <= 132 for ln in lines)
+    code = [ln.split("!")[0].strip().lower() for ln in lines]
+    opened = sum(1 for ln in code if re.match(r"(integer\(c_int\)|type\(c_ptr\)) function ", ln)
+                 or re.match(r"function ", ln))
+    closed = sum(1 for ln in code if ln == "end function")
+    assert opened == closed > 0
+    assert code.count("interface") == 1 and code.count("end interface") == 1
+    assert sum(ln.startswith("module z2_cuda_mod") for ln in code) == 1
+    assert sum(ln.startswith("end module z2_cuda_mod") for ln in code) == 1
+    # continuation lines end with '&' and are followed by a line
+    for i, ln in enumerate(code):
+        if ln.endswith("&"):
+            assert i + 1 < len(code) and code[i + 1]

@@ -30,7 +30,18 @@ EXPORTS = (
     "z2_stab_UR", "z2_stab_UL", "z2_stab_green", "z2_stab_green_big",
     "z2_stab_green_noalloc", "z2_get_phase_cycles", "z2_tune_delay", "z2_get_obs_tau_k",
     "z2_sweep_global", "z2_get_global_stats", "z2_therm",
+    # module-level mirrors on a chain's resident state
+    "z2_propK_pre", "z2_propK_L", "z2_propK_R", "z2_propgrK_R", "z2_propT_pre", "z2_propT_L",
+    "z2_propT_R", "z2_propgrT_R", "z2_wrap_pre", "z2_wrap_L", "z2_wrap_R", "z2_wrap_tau",
+    "z2_dyn_reset", "z2_prop_slice_L", "z2_prop_slice_R", "z2_sweep_reset",
+    "z2_obs_equal_calc", "z2_obs_equal_ave", "z2_obs_tau_calc", "z2_obs_tau_ave",
+    "z2_get_prop", "z2_set_prop", "z2_get_propgr",
 )
+# entry points (handle, chain, nt) and (handle, chain) of the state mirrors
+STATE_NT = ("z2_propK_pre", "z2_propK_L", "z2_propK_R", "z2_propgrK_R", "z2_wrap_pre",
+            "z2_wrap_tau", "z2_prop_slice_L", "z2_prop_slice_R", "z2_obs_equal_calc",
+            "z2_obs_tau_calc")
+STATE_CHAIN = ("z2_propT_pre", "z2_propT_L", "z2_propT_R", "z2_propgrT_R", "z2_dyn_reset")
 Z2_NOALLOC_NMAX = 144
 
 
@@ -102,7 +113,19 @@ def load():
         "z2_get_global_stats": (C.c_int, [vp, i32, dp]),
         "z2_tune_delay": (C.c_int, [C.POINTER(ChainParams), i32, C.POINTER(Options),
                                    C.POINTER(i32)]),
+        "z2_wrap_L": (C.c_int, [vp, i32, i32, i32]),
+        "z2_wrap_R": (C.c_int, [vp, i32, i32, i32]),
+        "z2_sweep_reset": (C.c_int, [vp, i32, i32]),
+        "z2_obs_equal_ave": (C.c_int, [vp, i32, i32]),
+        "z2_obs_tau_ave": (C.c_int, [vp, i32, i32]),
+        "z2_get_prop": (C.c_int, [vp, i32, dp, dp, dp, dp, dp, dp, dp]),
+        "z2_set_prop": (C.c_int, [vp, i32, dp, dp, dp, dp, dp, dp, dp]),
+        "z2_get_propgr": (C.c_int, [vp, i32, dp, dp, dp, dp]),
     }
+    for name in STATE_NT:
+        sig[name] = (C.c_int, [vp, i32, i32])
+    for name in STATE_CHAIN:
+        sig[name] = (C.c_int, [vp, i32])
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
         f.restype = res

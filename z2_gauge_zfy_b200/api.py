@@ -351,3 +351,97 @@ class Z2Batch:
         self._c(self.lib.z2_stab_green_big(self.h, chain, *[dptr(a) for a in args],
                                            *[dptr(o) for o in outs]))
         return tuple(o.reshape(n, n).T.copy() for o in outs)
+
+    # -- module-level mirrors on a chain's resident state -----------------------
+    # (src/multiply.f90, src/stabilization.f90:374-514, src/dynamics.f90:41-48,
+    # src/localK.f90:347-398, src/local_sweep.f90:56-71, src/obser_equal.f90,
+    # src/obser_tau.f90); nt follows the reference (1..Ltrot, wraps 0..Ltrot)
+    def propK_pre(self, chain: int, nt: int):
+        self._c(self.lib.z2_propK_pre(self.h, chain, nt))
+
+    def propK_L(self, chain: int, nt: int):
+        self._c(self.lib.z2_propK_L(self.h, chain, nt))
+
+    def propK_R(self, chain: int, nt: int):
+        self._c(self.lib.z2_propK_R(self.h, chain, nt))
+
+    def propgrK_R(self, chain: int, nt: int):
+        self._c(self.lib.z2_propgrK_R(self.h, chain, nt))
+
+    def propT_pre(self, chain: int):
+        self._c(self.lib.z2_propT_pre(self.h, chain))
+
+    def propT_L(self, chain: int):
+        self._c(self.lib.z2_propT_L(self.h, chain))
+
+    def propT_R(self, chain: int):
+        self._c(self.lib.z2_propT_R(self.h, chain))
+
+    def propgrT_R(self, chain: int):
+        self._c(self.lib.z2_propgrT_R(self.h, chain))
+
+    def wrap_pre(self, chain: int, nt: int):
+        self._c(self.lib.z2_wrap_pre(self.h, chain, nt))
+
+    def wrap_L(self, chain: int, nt: int, flag: bool = True):
+        self._c(self.lib.z2_wrap_L(self.h, chain, nt, 1 if flag else 0))
+
+    def wrap_R(self, chain: int, nt: int, flag: bool = True):
+        self._c(self.lib.z2_wrap_R(self.h, chain, nt, 1 if flag else 0))
+
+    def wrap_tau(self, chain: int, nt: int):
+        self._c(self.lib.z2_wrap_tau(self.h, chain, nt))
+
+    def dyn_reset(self, chain: int):
+        self._c(self.lib.z2_dyn_reset(self.h, chain))
+
+    def prop_slice_L(self, chain: int, nt: int):
+        self._c(self.lib.z2_prop_slice_L(self.h, chain, nt))
+
+    def prop_slice_R(self, chain: int, nt: int):
+        self._c(self.lib.z2_prop_slice_R(self.h, chain, nt))
+
+    def sweep_reset(self, chain: int, toggle: bool = False):
+        self._c(self.lib.z2_sweep_reset(self.h, chain, 1 if toggle else 0))
+
+    def obs_equal_calc(self, chain: int, nt: int):
+        self._c(self.lib.z2_obs_equal_calc(self.h, chain, nt))
+
+    def obs_equal_ave(self, chain: int, nobs: int):
+        self._c(self.lib.z2_obs_equal_ave(self.h, chain, nobs))
+
+    def obs_tau_calc(self, chain: int, nt: int):
+        self._c(self.lib.z2_obs_tau_calc(self.h, chain, nt))
+
+    def obs_tau_ave(self, chain: int, nobst: int):
+        self._c(self.lib.z2_obs_tau_ave(self.h, chain, nobst))
+
+    def get_prop(self, chain: int) -> dict:
+        """The Propagator: G, UR, DR, VR, UL, DL, VL (natural indexing)."""
+        N = self.dims(chain)[0]
+        m = {k: np.empty(N * N) for k in ("G", "UR", "VR", "UL", "VL")}
+        d = {k: np.empty(N) for k in ("DR", "DL")}
+        self._c(self.lib.z2_get_prop(self.h, chain, dptr(m["G"]), dptr(m["UR"]), dptr(d["DR"]),
+                                     dptr(m["VR"]), dptr(m["UL"]), dptr(d["DL"]),
+                                     dptr(m["VL"])))
+        out = {k: v.reshape(N, N).T.copy() for k, v in m.items()}
+        out.update(d)
+        return out
+
+    def set_prop(self, chain: int, G=None, UR=None, DR=None, VR=None, UL=None, DL=None,
+                 VL=None):
+        """Load any of the Propagator's matrices (None leaves one unchanged)."""
+        given = {k: v for k, v in dict(G=G, UR=UR, DR=DR, VR=VR, UL=UL, DL=DL, VL=VL).items()
+                 if v is not None}
+        bufs = dict(zip(given, self._mats(chain, **given)))
+        ptr = {k: (dptr(bufs[k]) if k in bufs else None)
+               for k in ("G", "UR", "DR", "VR", "UL", "DL", "VL")}
+        self._c(self.lib.z2_set_prop(self.h, chain, ptr["G"], ptr["UR"], ptr["DR"], ptr["VR"],
+                                     ptr["UL"], ptr["DL"], ptr["VL"]))
+
+    def get_propgr(self, chain: int) -> dict:
+        """PropGreen of the time-displaced chain: G00, G0t, Gt0, Gtt."""
+        N = self.dims(chain)[0]
+        m = {k: np.empty(N * N) for k in ("G00", "G0t", "Gt0", "Gtt")}
+        self._c(self.lib.z2_get_propgr(self.h, chain, *[dptr(v) for v in m.values()]))
+        return {k: v.reshape(N, N).T.copy() for k, v in m.items()}

@@ -71,6 +71,9 @@ z2_chain_kernel(const ChainDesc *descs, const int *order, int nchains, int *queu
   }
 }
 
+__global__ void __launch_bounds__(Z2_NT, 1)
+z2_state_kernel(const ChainDesc *desc, int op, int nt, int flag, double x, unsigned smem_bytes);
+
 // Module-level mirrors on single matrices, one CTA.
 __global__ void __launch_bounds__(Z2_NT, 1)
 z2_unit_kernel(const ChainDesc *desc, int op, UnitArgs a, unsigned smem_bytes) {
@@ -429,6 +432,8 @@ extern "C" int z2_create(z2_handle **out, const z2_chain_params *params, int32_t
   CUDA_TRY(h, cudaFuncSetAttribute(z2_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)h->smem));
   CUDA_TRY(h, cudaFuncSetAttribute(z2_unit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)h->smem));
+  CUDA_TRY(h, cudaFuncSetAttribute(z2_state_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)h->smem));
   CUDA_TRY(h, cudaMalloc(&h->d_status, sizeof(int) * nchains));
   CUDA_TRY(h, cudaMemset(h->d_status, 0, sizeof(int) * nchains));
@@ -1223,6 +1228,307 @@ extern "C" int z2_stab_green_big(z2_handle *h, int32_t chain, const double *UR, 
   CUDA_TRY(h, cudaMemcpy(G0t, a.G0t, NN * 8, cudaMemcpyDeviceToHost));
   CUDA_TRY(h, cudaMemcpy(Gt0, a.Gt0, NN * 8, cudaMemcpyDeviceToHost));
   CUDA_TRY(h, cudaMemcpy(Gtt, a.Gtt, NN * 8, cudaMemcpyDeviceToHost));
+  return Z2_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Module-level mirrors on a chain's resident state.  Each entry point runs one
+// procedure of the reference's multiply / stabilization / dynamics /
+// obser_equal / obser_tau / localK modules on one chain of the handle, on the
+// state the handle keeps in global memory between calls (the Propagator G,
+// UR DR VR, UL DL VL, the UDV stacks, the Dyn copy and PropGreen, sigma, the
+// ranf state and the observable sums), so that a driver can replace the
+// reference's modules one at a time.  The U factors are propagated at every
+// call (the whole-bin path propagates them lazily, with the same operations in
+// the same order).  One CTA, the chain kernel's shared-memory plan.
+// ---------------------------------------------------------------------------
+enum {
+  SO_PROPK_PRE = 1, SO_PROPT_PRE, SO_PROPK_L, SO_PROPK_R, SO_PROPT_L, SO_PROPT_R,
+  SO_PROPGRK_R, SO_PROPGRT_R, SO_WRAP_PRE, SO_WRAP_L, SO_WRAP_R, SO_WRAP_TAU,
+  SO_DYN_RESET, SO_SWEEP_RESET, SO_OBS_EQ_CALC, SO_OBS_EQ_AVE, SO_OBS_TAU_CALC,
+  SO_OBS_TAU_AVE, SO_SLICE_L, SO_SLICE_R
+};
+
+__global__ void __launch_bounds__(Z2_NT, 1)
+z2_state_kernel(const ChainDesc *desc, int op, int nt, int flag, double x, unsigned smem_bytes) {
+  extern __shared__ __align__(16) unsigned char z2_smem[];
+  __shared__ ChainDesc sc;
+  __shared__ Smem s;
+  load_desc(sc, desc);
+  if (threadIdx.x == 0) s = make_smem(sc, z2_smem, smem_bytes);
+  __syncthreads();
+  const ChainDesc &c = sc;
+  const int N = c.N;
+  Pend pd{1, 0};
+  switch (op) {
+    case SO_PROPK_PRE:      // propK_pre (src/multiply.f90:8-15) as Local_sweep_pre calls it
+      if (c.use_kin) { build_table(c, s, nt); kin_global(c, s, c.UR, 1, 0); }
+      break;
+    case SO_PROPT_PRE:      // propT_pre (src/multiply.f90:65-77)
+      blk_scale(c.UR, N, N, N, c.eP);
+      break;
+    case SO_PROPK_L:        // propK_L (src/multiply.f90:17-28): G B, B^-1 G, UL B
+      load_G(c, s);
+      build_table(c, s, nt);
+      kin_cols(c, s, s.G, s.ldg, N, 1);
+      kin_rows(c, s, s.G, s.ldg, N, -1);
+      spill_G(c, s);
+      kin_global(c, s, c.ULT, 1, 0);      // UL^T <- B UL^T (B symmetric)
+      break;
+    case SO_PROPK_R:        // propK_R (src/multiply.f90:30-41): B G, G B^-1, B UR
+      load_G(c, s);
+      build_table(c, s, nt);
+      kin_rows(c, s, s.G, s.ldg, N, 1);
+      kin_cols(c, s, s.G, s.ldg, N, -1);
+      spill_G(c, s);
+      kin_global(c, s, c.UR, 1, 0);
+      break;
+    case SO_PROPT_L:        // propT_L (src/multiply.f90:79-93)
+      blk_scale(c.G, N, N, N, c.eP);
+      blk_scale(c.G, N, N, N, c.eM);
+      blk_scale(c.ULT, N, N, N, c.eP);
+      break;
+    case SO_PROPT_R:        // propT_R (src/multiply.f90:95-108)
+      blk_scale(c.G, N, N, N, c.eP);
+      blk_scale(c.G, N, N, N, c.eM);
+      blk_scale(c.UR, N, N, N, c.eP);
+      break;
+    case SO_PROPGRK_R:      // propgrK_R (src/multiply.f90:43-63) on the Dyn copy
+      if (c.use_kin) {
+        propgr_R(c, s, nt, true, false);
+        kin_global(c, s, c.URd, 1, 0);
+      }
+      break;
+    case SO_PROPGRT_R:      // propgrT_R (src/multiply.f90:110-130)
+      propgr_R(c, s, nt, false, true);
+      blk_scale(c.URd, N, N, N, c.eP);
+      break;
+    case SO_WRAP_PRE:       // Wrap_pre (src/stabilization.f90:374-398)
+      wrap_pre(c, s, nt, pd);
+      break;
+    case SO_WRAP_L:         // Wrap_L (src/stabilization.f90:400-437)
+      load_G(c, s);
+      wrap_L(c, s, nt, pd, flag != 0);
+      spill_G(c, s);
+      break;
+    case SO_WRAP_R:         // Wrap_R (src/stabilization.f90:439-476)
+      load_G(c, s);
+      wrap_R(c, s, nt, pd, flag != 0);
+      spill_G(c, s);
+      break;
+    case SO_WRAP_TAU:       // Wrap_tau (src/stabilization.f90:478-514)
+      wrap_tau(c, s, nt, pd);
+      break;
+    case SO_DYN_RESET:      // Dyn_reset (src/dynamics.f90:41-48)
+      dyn_reset(c, s);
+      break;
+    case SO_SWEEP_RESET:    // Local_sweep_reset (src/local_sweep.f90:56-71)
+      sweep_reset(c, flag != 0, c.hzero != 0);
+      break;
+    case SO_OBS_EQ_CALC:    // Obs_equal%calc (src/obser_equal.f90:73-149)
+      load_G(c, s);
+      obs_equal(c, s, nt);
+      break;
+    case SO_OBS_EQ_AVE:     // Obs_equal%ave (src/obser_equal.f90:50-71)
+      obs_equal_ave(c, x);
+      break;
+    case SO_OBS_TAU_CALC:   // Obs_tau%calc (src/obser_tau.f90:56-133)
+      obs_tau(c, s, nt);
+      break;
+    case SO_OBS_TAU_AVE:    // Obs_tau%ave (src/obser_tau.f90:37-47)
+      obs_tau_ave(c, x);
+      break;
+    case SO_SLICE_L:        // LocalK_prop_L (src/localK.f90:347-373)
+    case SO_SLICE_R:        // LocalK_prop_R (src/localK.f90:375-398)
+      for (int i = threadIdx.x; i < 2 * c.nb; i += Z2_NT) s.bond[i] = c.bonds[i];
+      __syncthreads();
+      load_G(c, s);
+      if (op == SO_SLICE_L) {
+        propose_slice(c, s, nt, true, 0);            // bonds 2N..1
+        build_table(c, s, nt);
+        kin_cols(c, s, s.G, s.ldg, N, 1);
+        kin_rows(c, s, s.G, s.ldg, N, -1);
+        spill_G(c, s);
+        kin_global(c, s, c.ULT, 1, 0);
+      } else {
+        build_table(c, s, nt);
+        kin_rows(c, s, s.G, s.ldg, N, 1);
+        kin_cols(c, s, s.G, s.ldg, N, -1);
+        propose_slice(c, s, nt, false, 1);           // bonds 1..2N
+        spill_G(c, s);
+        build_table(c, s, nt);                       // B_nt with the flipped links
+        kin_global(c, s, c.UR, 1, 0);
+      }
+      break;
+    default:
+      break;
+  }
+}
+
+// Launch one state procedure on one chain, synchronously; a non-finite drift
+// or Green's function found by it is Z2_ERR_NONFINITE.
+static int run_state(z2_handle *h, int chain, int op, int nt, int flag, double x) {
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  z2_state_kernel<<<1, Z2_NT, h->smem, h->stream>>>(h->d_desc + chain, op, nt, flag, x, h->smem);
+  CUDA_TRY(h, cudaGetLastError());
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  int st = 0;
+  CUDA_TRY(h, cudaMemcpy(&st, h->d_status + chain, sizeof(int), cudaMemcpyDeviceToHost));
+  if (st & ST_NONFINITE) return set_err(h, Z2_ERR_NONFINITE, "chain %d: non-finite Green's function", chain);
+  return Z2_OK;
+}
+
+// nt of a per-slice procedure: 1..Ltrot.
+static int slice_op(z2_handle *h, int chain, int nt, int op, const char *fn) {
+  int r = check_chain(h, chain);
+  if (r) return r;
+  if (nt < 1 || nt > h->ch[chain].Ltrot)
+    return set_err(h, Z2_ERR_ARG, "%s: nt = %d out of 1..Ltrot", fn, nt);
+  return run_state(h, chain, op, nt, 0, 0.0);
+}
+
+// nt of a wrap: a stabilization point 0..Ltrot (a multiple of Nwrap).
+static int wrap_op(z2_handle *h, int chain, int nt, int flag, int op, const char *fn, int lo) {
+  int r = check_chain(h, chain);
+  if (r) return r;
+  const ChainHost &C = h->ch[chain];
+  if (nt < lo || nt > C.Ltrot || nt % C.p.Nwrap != 0)
+    return set_err(h, Z2_ERR_ARG, "%s: nt = %d is not a stabilization point (%d..Ltrot, a multiple "
+                   "of Nwrap)", fn, nt, lo);
+  r = run_state(h, chain, op, nt, flag, 0.0);
+  if (r == Z2_OK && op == SO_WRAP_PRE && nt == C.Ltrot) h->pre_done = true;
+  return r;
+}
+
+static int chain_op(z2_handle *h, int chain, int op, int flag, double x) {
+  int r = check_chain(h, chain);
+  if (r) return r;
+  return run_state(h, chain, op, 0, flag, x);
+}
+
+extern "C" int z2_propK_pre(z2_handle *h, int32_t chain, int32_t nt) {
+  return slice_op(h, chain, nt, SO_PROPK_PRE, "z2_propK_pre");
+}
+extern "C" int z2_propK_L(z2_handle *h, int32_t chain, int32_t nt) {
+  return slice_op(h, chain, nt, SO_PROPK_L, "z2_propK_L");
+}
+extern "C" int z2_propK_R(z2_handle *h, int32_t chain, int32_t nt) {
+  return slice_op(h, chain, nt, SO_PROPK_R, "z2_propK_R");
+}
+extern "C" int z2_propgrK_R(z2_handle *h, int32_t chain, int32_t nt) {
+  return slice_op(h, chain, nt, SO_PROPGRK_R, "z2_propgrK_R");
+}
+extern "C" int z2_propT_pre(z2_handle *h, int32_t chain) { return chain_op(h, chain, SO_PROPT_PRE, 0, 0.0); }
+extern "C" int z2_propT_L(z2_handle *h, int32_t chain) { return chain_op(h, chain, SO_PROPT_L, 0, 0.0); }
+extern "C" int z2_propT_R(z2_handle *h, int32_t chain) { return chain_op(h, chain, SO_PROPT_R, 0, 0.0); }
+extern "C" int z2_propgrT_R(z2_handle *h, int32_t chain) {
+  return chain_op(h, chain, SO_PROPGRT_R, 0, 0.0);
+}
+extern "C" int z2_wrap_pre(z2_handle *h, int32_t chain, int32_t nt) {
+  return wrap_op(h, chain, nt, 0, SO_WRAP_PRE, "z2_wrap_pre", 0);
+}
+extern "C" int z2_wrap_L(z2_handle *h, int32_t chain, int32_t nt, int32_t flag) {
+  return wrap_op(h, chain, nt, flag, SO_WRAP_L, "z2_wrap_L", 0);
+}
+extern "C" int z2_wrap_R(z2_handle *h, int32_t chain, int32_t nt, int32_t flag) {
+  return wrap_op(h, chain, nt, flag, SO_WRAP_R, "z2_wrap_R", 0);
+}
+extern "C" int z2_wrap_tau(z2_handle *h, int32_t chain, int32_t nt) {
+  return wrap_op(h, chain, nt, 0, SO_WRAP_TAU, "z2_wrap_tau", 1);
+}
+extern "C" int z2_dyn_reset(z2_handle *h, int32_t chain) { return chain_op(h, chain, SO_DYN_RESET, 0, 0.0); }
+extern "C" int z2_sweep_reset(z2_handle *h, int32_t chain, int32_t toggle) {
+  return chain_op(h, chain, SO_SWEEP_RESET, toggle != 0, 0.0);
+}
+extern "C" int z2_obs_equal_calc(z2_handle *h, int32_t chain, int32_t nt) {
+  return slice_op(h, chain, nt, SO_OBS_EQ_CALC, "z2_obs_equal_calc");
+}
+extern "C" int z2_obs_equal_ave(z2_handle *h, int32_t chain, int32_t nobs) {
+  if (nobs < 0) return set_err(h, Z2_ERR_ARG, "z2_obs_equal_ave: nobs = %d", nobs);
+  return chain_op(h, chain, SO_OBS_EQ_AVE, 0, (double)nobs);
+}
+extern "C" int z2_obs_tau_calc(z2_handle *h, int32_t chain, int32_t nt) {
+  return slice_op(h, chain, nt, SO_OBS_TAU_CALC, "z2_obs_tau_calc");
+}
+extern "C" int z2_obs_tau_ave(z2_handle *h, int32_t chain, int32_t nobst) {
+  if (nobst < 1) return set_err(h, Z2_ERR_ARG, "z2_obs_tau_ave: nobst = %d", nobst);
+  return chain_op(h, chain, SO_OBS_TAU_AVE, 0, (double)nobst);
+}
+extern "C" int z2_prop_slice_L(z2_handle *h, int32_t chain, int32_t nt) {
+  return slice_op(h, chain, nt, SO_SLICE_L, "z2_prop_slice_L");
+}
+extern "C" int z2_prop_slice_R(z2_handle *h, int32_t chain, int32_t nt) {
+  return slice_op(h, chain, nt, SO_SLICE_R, "z2_prop_slice_R");
+}
+
+// Propagator readback / upload: G, UR DR VR, UL DL VL (UL in the reference's
+// orientation; the handle keeps UL^T).  Each buffer is optional.
+extern "C" int z2_get_prop(const z2_handle *h, int32_t chain, double *G, double *UR, double *DR,
+                           double *VR, double *UL, double *DL, double *VL) {
+  int r = check_chain(h, chain);
+  if (r) return r;
+  z2_handle *hh = const_cast<z2_handle *>(h);
+  const ChainHost &C = h->ch[chain];
+  const int N = C.N;
+  const size_t NN = (size_t)N * N;
+  CUDA_TRY(hh, cudaSetDevice(h->device));
+  auto get = [&](double *dst, const double *src, size_t n) {
+    return dst ? cudaMemcpy(dst, src, n * 8, cudaMemcpyDeviceToHost) : cudaSuccess;
+  };
+  CUDA_TRY(hh, get(G, C.d.G, NN));
+  CUDA_TRY(hh, get(UR, C.d.UR, NN));
+  CUDA_TRY(hh, get(DR, C.d.DR, N));
+  CUDA_TRY(hh, get(VR, C.d.VR, NN));
+  CUDA_TRY(hh, get(DL, C.d.DL, N));
+  CUDA_TRY(hh, get(VL, C.d.VL, NN));
+  if (UL) {
+    std::vector<double> t(NN);
+    CUDA_TRY(hh, cudaMemcpy(t.data(), C.d.ULT, NN * 8, cudaMemcpyDeviceToHost));
+    transpose_host(t.data(), UL, N);
+  }
+  return Z2_OK;
+}
+
+extern "C" int z2_set_prop(z2_handle *h, int32_t chain, const double *G, const double *UR,
+                           const double *DR, const double *VR, const double *UL, const double *DL,
+                           const double *VL) {
+  int r = check_chain(h, chain);
+  if (r) return r;
+  const ChainHost &C = h->ch[chain];
+  const int N = C.N;
+  const size_t NN = (size_t)N * N;
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  auto put = [&](double *dst, const double *src, size_t n) {
+    return src ? cudaMemcpy(dst, src, n * 8, cudaMemcpyHostToDevice) : cudaSuccess;
+  };
+  CUDA_TRY(h, put(C.d.G, G, NN));
+  CUDA_TRY(h, put(C.d.UR, UR, NN));
+  CUDA_TRY(h, put(C.d.DR, DR, N));
+  CUDA_TRY(h, put(C.d.VR, VR, NN));
+  CUDA_TRY(h, put(C.d.DL, DL, N));
+  CUDA_TRY(h, put(C.d.VL, VL, NN));
+  if (UL) {
+    std::vector<double> t(NN);
+    transpose_host(UL, t.data(), N);
+    CUDA_TRY(h, cudaMemcpy(C.d.ULT, t.data(), NN * 8, cudaMemcpyHostToDevice));
+  }
+  return Z2_OK;
+}
+
+// PropGreen readback (src/process_matrix.f90:14-20): Gr00, Gr0t, Grt0, Grtt
+// of the time-displaced chain; each buffer optional.
+extern "C" int z2_get_propgr(const z2_handle *h, int32_t chain, double *G00, double *G0t,
+                             double *Gt0, double *Gtt) {
+  int r = check_chain(h, chain);
+  if (r) return r;
+  z2_handle *hh = const_cast<z2_handle *>(h);
+  const ChainHost &C = h->ch[chain];
+  const size_t NN = (size_t)C.N * C.N;
+  CUDA_TRY(hh, cudaSetDevice(h->device));
+  const double *src[4] = {C.d.G00, C.d.G0t, C.d.Gt0, C.d.Gtt};
+  double *dst[4] = {G00, G0t, Gt0, Gtt};
+  for (int q = 0; q < 4; ++q)
+    if (dst[q]) CUDA_TRY(hh, cudaMemcpy(dst[q], src[q], NN * 8, cudaMemcpyDeviceToHost));
   return Z2_OK;
 }
 

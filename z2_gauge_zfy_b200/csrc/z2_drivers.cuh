@@ -32,9 +32,10 @@ __device__ __noinline__ void wrap_tau(const ChainDesc &c, const Smem &s, int nt,
   green_big_extract(N, T, c.G00, c.G0t, c.Gt0, c.Gtt);
 }
 
-// Dyn_reset + Dyn_sweep_R (src/dynamics.f90:41-62): the G(tau,0) chain.
-// The arena is free here (G is spilled in c.G).
-__device__ __noinline__ void dyn_sweep(const ChainDesc &c, const Smem &s) {
+// Dyn_reset (src/dynamics.f90:41-48, Propgr_reset src/process_matrix.f90:88-96):
+// the Dyn copy of the propagator and G00 = Gtt = Gt0 = G, G0t = -(I - G),
+// from the chain's G in global memory.
+__device__ __noinline__ void dyn_reset(const ChainDesc &c, const Smem &s) {
   const int N = c.N;
   blk_copy(c.URd, N, c.UR, N, N, N);
   blk_copy(c.VRd, N, c.VR, N, N, N);
@@ -52,21 +53,35 @@ __device__ __noinline__ void dyn_sweep(const ChainDesc &c, const Smem &s) {
       c.G0t[i + (size_t)j * N] = -((i == j ? 1.0 : 0.0) - g);
     }
   __syncthreads();
+}
+
+// propgrK_R (src/multiply.f90:43-63) without the U factor, and propgrT_R
+// (src/multiply.f90:110-130): Gt0 <- B Gt0, G0t <- G0t B^-1, Gtt <- B Gtt B^-1,
+// then the mu factors.
+__device__ __noinline__ void propgr_R(const ChainDesc &c, const Smem &s, int nt, bool kin, bool mu) {
+  const int N = c.N;
+  if (kin && c.use_kin) {
+    build_table(c, s, nt);
+    kin_global(c, s, c.Gt0, 1, 0);
+    kin_global(c, s, c.G0t, 0, -1);
+    kin_global(c, s, c.Gtt, 1, -1);
+  }
+  if (mu && (c.eP != 1.0 || c.eM != 1.0)) {
+    blk_scale(c.Gt0, N, N, N, c.eP);
+    blk_scale(c.G0t, N, N, N, c.eM);
+    blk_scale(c.Gtt, N, N, N, c.eP);
+    blk_scale(c.Gtt, N, N, N, c.eM);
+  }
+}
+
+// Dyn_reset + Dyn_sweep_R (src/dynamics.f90:41-62): the G(tau,0) chain.
+// The arena is free here (G is spilled in c.G).
+__device__ __noinline__ void dyn_sweep(const ChainDesc &c, const Smem &s) {
+  dyn_reset(c, s);
   Pend pd{1, 0};
   for (int nt = 1; nt <= c.Ltrot; ++nt) {
     obs_tau(c, s, nt);
-    if (c.use_kin) {      // propgrK_R (src/multiply.f90:43-63)
-      build_table(c, s, nt);
-      kin_global(c, s, c.Gt0, 1, 0);
-      kin_global(c, s, c.G0t, 0, -1);
-      kin_global(c, s, c.Gtt, 1, -1);
-    }
-    if (c.eP != 1.0 || c.eM != 1.0) {   // propgrT_R (src/multiply.f90:110-130)
-      blk_scale(c.Gt0, N, N, N, c.eP);
-      blk_scale(c.G0t, N, N, N, c.eM);
-      blk_scale(c.Gtt, N, N, N, c.eP);
-      blk_scale(c.Gtt, N, N, N, c.eM);
-    }
+    propgr_R(c, s, nt, true, true);
     if (pd.lo > pd.hi) { pd.lo = nt; pd.hi = nt; } else pd.hi = nt;
     if (nt % c.Nwrap == 0) wrap_tau(c, s, nt, pd);
   }
@@ -147,11 +162,13 @@ __device__ __noinline__ void sweep_R(const ChainDesc &c, const Smem &s, bool tog
   }
 }
 
-// Local_sweep (src/local_sweep.f90:152-195): one bin.
-__device__ __noinline__ void chain_sweep(const ChainDesc &c, const Smem &s, int nsweep, bool toggle,
-                            double h_is_zero) {
+__device__ __noinline__ void bin_average(const ChainDesc &c, bool toggle);
+
+// Local_sweep_reset (src/local_sweep.f90:56-71): the bin's sums and
+// acceptance counters, the tau correlators when toggle, and for h = 0 the
+// links made constant in tau.
+__device__ __noinline__ void sweep_reset(const ChainDesc &c, bool toggle, bool h_is_zero) {
   const int N = c.N;
-  // Local_sweep_reset (src/local_sweep.f90:56-71)
   if (threadIdx.x == 0) {
     for (int q = A_FLUX_SUM; q <= A_ACC_DEN; ++q) c.acc[q] = 0.0;
   }
@@ -159,12 +176,19 @@ __device__ __noinline__ void chain_sweep(const ChainDesc &c, const Smem &s, int 
     const size_t n = (size_t)7 * c.Ltrot * N;
     for (size_t i = threadIdx.x; i < n; i += Z2_NT) c.obs_tau[i] = 0.0;
   }
-  if (h_is_zero != 0.0) {
+  if (h_is_zero) {
     for (int b = threadIdx.x; b < c.nb; b += Z2_NT) {
       signed char v = c.sigma[b];
       for (int t = 1; t < c.Ltrot; ++t) c.sigma[(size_t)t * c.nb + b] = v;
     }
   }
+  __syncthreads();
+}
+
+// Local_sweep (src/local_sweep.f90:152-195): one bin.
+__device__ __noinline__ void chain_sweep(const ChainDesc &c, const Smem &s, int nsweep, bool toggle,
+                            double h_is_zero) {
+  sweep_reset(c, toggle, h_is_zero != 0.0);
   for (int i = threadIdx.x; i < 2 * c.nb; i += Z2_NT) s.bond[i] = c.bonds[i];
   __syncthreads();
   load_G(c, s);
@@ -177,9 +201,14 @@ __device__ __noinline__ void chain_sweep(const ChainDesc &c, const Smem &s, int 
       sweep_L(c, s);
     }
   }
+  bin_average(c, toggle);
+}
+
+// Obs_equal_ave (src/obser_equal.f90:50-71): the bin averages of nobs
+// slices into the chain's readback slots.
+__device__ __noinline__ void obs_equal_ave(const ChainDesc &c, double nobs) {
+  const int N = c.N;
   if (threadIdx.x == 0) {
-    // Obs_equal_ave (src/obser_equal.f90:50-71)
-    const double nobs = c.acc[A_NOBS];
     double *o = c.acc + A_BIN0;
     for (int q = 0; q < 7; ++q) o[q] = 0.0;
     if (nobs > 0.0) {
@@ -193,15 +222,25 @@ __device__ __noinline__ void chain_sweep(const ChainDesc &c, const Smem &s, int 
       o[5] = (o[3] > 1.0e-12) ? 1.0 - o[4] / o[3] : 0.0;
       o[6] = c.acc[A_DENS] * z;
     }
-    // Acc_calc_ratio (src/process_matrix.f90:134-140)
-    if (c.acc[A_ACC_DEN] > 0.0) c.acc[A_ACC] += c.acc[A_ACC_NUM] / c.acc[A_ACC_DEN];
   }
-  if (toggle) {   // Obs_tau_ave (src/obser_tau.f90:37-47)
-    __syncthreads();
-    const double z = 1.0 / c.acc[A_NOBST];
-    const size_t n = (size_t)7 * c.Ltrot * N;
-    for (size_t i = threadIdx.x; i < n; i += Z2_NT) c.obs_tau[i] = z * c.obs_tau[i];
-  }
+  __syncthreads();
+}
+
+// Obs_tau_ave (src/obser_tau.f90:37-47): the tau correlators / nobst.
+__device__ __noinline__ void obs_tau_ave(const ChainDesc &c, double nobst) {
+  const double z = 1.0 / nobst;
+  const size_t n = (size_t)7 * c.Ltrot * c.N;
+  for (size_t i = threadIdx.x; i < n; i += Z2_NT) c.obs_tau[i] = z * c.obs_tau[i];
+  __syncthreads();
+}
+
+// End of a bin: Obs_equal_ave, Acc_calc_ratio (src/process_matrix.f90:134-140)
+// and, with toggle, Obs_tau_ave, with the counts the half-sweeps kept.
+__device__ __noinline__ void bin_average(const ChainDesc &c, bool toggle) {
+  obs_equal_ave(c, c.acc[A_NOBS]);
+  if (threadIdx.x == 0 && c.acc[A_ACC_DEN] > 0.0)
+    c.acc[A_ACC] += c.acc[A_ACC_NUM] / c.acc[A_ACC_DEN];
+  if (toggle) obs_tau_ave(c, c.acc[A_NOBST]);
   __syncthreads();
 }
 
