@@ -19,6 +19,7 @@ module z2_cuda_mod
     type, bind(C) :: z2_options
         integer(c_int32_t) :: delay_k, record, device, tau, graph
         type(c_ptr)     :: delay_k_chain    ! c_null_ptr, or c_loc(k(1)) from z2_tune_delay
+        integer(c_int32_t) :: stab_exact    ! 1 = the reference's pivoted QR in the wraps
     end type
     interface
         integer(c_int) function z2_create(h, p, n, opt) bind(C, name="z2_create")

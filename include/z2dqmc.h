@@ -76,6 +76,12 @@ typedef struct z2_options {
   int32_t tau;       /* 1: allocate the time-displaced chain (is_tau) */
   int32_t graph;     /* 1: capture each bin's launch as a CUDA graph, replayed */
   const int32_t *delay_k_chain;  /* optional [nchains] per-chain delay rank (autotuner) */
+  int32_t stab_exact;  /* 1: stabilize with the reference's column-pivoted QR
+                          (ZGEQP3) and its stab_green branches; 0: pre-pivoted
+                          blocked QR and the scale-split Green's function (the
+                          same U D V products and G up to rounding, faster on
+                          the GPU).  The module-level z2_stab_* mirrors always
+                          use the reference's pivoted QR. */
 } z2_options;
 
 typedef struct z2_handle z2_handle;

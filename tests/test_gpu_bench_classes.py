@@ -36,12 +36,15 @@ def rel(a, b):
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
 
 
-def test_bench_classes_whole_bin_match_c_port():
+@pytest.mark.parametrize("stab_exact", [False, True], ids=["prepivoted", "pivoted"])
+def test_bench_classes_whole_bin_match_c_port(stab_exact):
+    """Both stabilizations: the pre-pivoted blocked QR with the scale-split G
+    (the default) and the reference's column-pivoted QR (stab_exact)."""
     chains = batched_chains()[:12] + single_chain()
     assert sorted({(c.Nlx, c.Ltrot) for c in chains[:12]}) == \
         [(L, Lt) for L in (6, 8, 10, 12) for Lt in (80, 120, 160)]
-    k = tune_delay(chains)
-    with Z2Batch(chains, record=True, delay_k_chain=k) as b:
+    k = tune_delay(chains, stab_exact=stab_exact)
+    with Z2Batch(chains, record=True, delay_k_chain=k, stab_exact=stab_exact) as b:
         b.pre()
         b.sweep(1, False)
         gpu = [dict(G=b.green(i), obs=b.obs_equal(i), st=b.stats(i), dec=b.decisions(i)[0],
@@ -69,4 +72,4 @@ def test_bench_classes_whole_bin_match_c_port():
         assert ex <= 1e-8, (tag, g["st"]["Xmaxm"], st["Xmaxm"])
         worst["G"] = max(worst["G"], eg)
         worst["Xmaxm"] = max(worst["Xmaxm"], ex)
-    print("worst relative differences:", worst)
+    print(f"stab_exact={stab_exact}: worst relative differences:", worst)

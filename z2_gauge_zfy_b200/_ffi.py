@@ -66,7 +66,7 @@ class Options(C.Structure):
     """``z2_options``."""
     _fields_ = [("delay_k", C.c_int32), ("record", C.c_int32), ("device", C.c_int32),
                 ("tau", C.c_int32), ("graph", C.c_int32),
-                ("delay_k_chain", C.POINTER(C.c_int32))]
+                ("delay_k_chain", C.POINTER(C.c_int32)), ("stab_exact", C.c_int32)]
 
 
 _lib = None

@@ -100,14 +100,14 @@ def _params(chains):
     return arr, keep
 
 
-def tune_delay(chains, device: int = 0) -> np.ndarray:
+def tune_delay(chains, device: int = 0, stab_exact: bool = False) -> np.ndarray:
     """Per-chain delayed-update rank picked by the library's autotuner
     (``z2_tune_delay``: short probe chains of each lattice size, timed at
     every candidate rank on the GPU)."""
     lib = _ffi.load()
     chains = list(chains)
     arr, _keep = _params(chains)
-    opt = Options(0, 0, device, 0, 0, None)
+    opt = Options(0, 0, device, 0, 0, None, 1 if stab_exact else 0)
     k = np.zeros(len(chains), dtype=np.int32)
     code = lib.z2_tune_delay(arr, len(chains), C.byref(opt),
                              k.ctypes.data_as(C.POINTER(C.c_int32)))
@@ -120,16 +120,19 @@ class Z2Batch:
     """A batch of chains resident on one GPU (``z2_create``)."""
 
     def __init__(self, chains, delay_k=0, record: bool = False, device: int = 0,
-                 tau: bool = False, graph: bool = False, delay_k_chain=None):
+                 tau: bool = False, graph: bool = False, delay_k_chain=None,
+                 stab_exact: bool = False):
         """delay_k: rank of the delayed updates for every chain (0 = built-in
         default per lattice size), or "auto" to run the autotuner
-        (``z2_tune_delay``) and use its per-chain ranks."""
+        (``z2_tune_delay``) and use its per-chain ranks.  stab_exact: stabilize
+        with the reference's column-pivoted QR instead of the pre-pivoted
+        blocked QR (``z2_options.stab_exact``)."""
         self.lib = _ffi.load()
         self.chains = list(chains)
         n = len(self.chains)
         arr, self._rt_keep = _params(self.chains)
         if delay_k == "auto":
-            delay_k_chain = tune_delay(self.chains, device)
+            delay_k_chain = tune_delay(self.chains, device, stab_exact)
             delay_k = 0
         self._kc = None
         kc_ptr = None
@@ -140,7 +143,7 @@ class Z2Batch:
                                  f"needs one rank per chain ({n},)")
             kc_ptr = self._kc.ctypes.data_as(C.POINTER(C.c_int32))
         opt = Options(delay_k, 1 if record else 0, device, 1 if tau else 0, 1 if graph else 0,
-                      kc_ptr)
+                      kc_ptr, 1 if stab_exact else 0)
         h = C.c_void_p()
         code = self.lib.z2_create(C.byref(h), arr, n, C.byref(opt))
         self.h = h

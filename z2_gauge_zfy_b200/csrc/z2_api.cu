@@ -328,6 +328,18 @@ static int smem_small_bytes(int N) {
   return (int)a16(off);
 }
 
+// Shared work space (doubles) a chain keeps after G and the delayed-update
+// factors: the GEMM staging minimum, the pre-pivoted QR's 64-column chunks,
+// and the blocked DORGQR with its parallel T prologue.
+static size_t tile_min(int N) {
+  const int ldv = qrf_ldv(N);
+  size_t t = kGemmTile;
+  t = std::max<size_t>(t, qrf_min_work(N));
+  t = std::max<size_t>(t, (size_t)ldv * 16 + 17 * (size_t)std::max(N - 16, 0));
+  t = std::max<size_t>(t, (size_t)Z2_WARPS * (2 * 16 * 16 + 4 * 16));
+  return t;
+}
+
 static int default_k(int N) {
   if (N <= 36) return 16;
   if (N <= 64) return 16;
@@ -401,16 +413,17 @@ extern "C" int z2_create(z2_handle **out, const z2_chain_params *params, int32_t
     size_t nn = (size_t)N * ldg;
     int g_in = 0;
     int k2 = 2 * k;
-    if (nn + std::max<size_t>(2 * (size_t)z2_ldx(N) * k2, kGemmTile) <= arena) g_in = 1;
-    else if (nn + std::max<size_t>(2 * (size_t)z2_ldx(N) * 4, kGemmTile) <= arena) {
+    const size_t tmin = tile_min(N);
+    if (nn + std::max<size_t>(2 * (size_t)z2_ldx(N) * k2, tmin) <= arena) g_in = 1;
+    else if (nn + std::max<size_t>(2 * (size_t)z2_ldx(N) * 4, tmin) <= arena) {
       g_in = 1;
       while (k2 > 4 && nn + 2 * (size_t)z2_ldx(N) * k2 > arena) k2 -= 2;
     }
     if (!g_in) {
       while (k2 > 2 && 2 * (size_t)z2_ldx(N) * k2 > arena) k2 -= 2;
     }
-    size_t need = small + 8 * (g_in ? nn + std::max<size_t>(2 * (size_t)z2_ldx(N) * k2, kGemmTile)
-                                    : std::max<size_t>(2 * (size_t)z2_ldx(N) * k2, kGemmTile));
+    size_t need = small + 8 * (g_in ? nn + std::max<size_t>(2 * (size_t)z2_ldx(N) * k2, tmin)
+                                    : std::max<size_t>(2 * (size_t)z2_ldx(N) * k2, tmin));
     smem_needed = std::max(smem_needed, (int)need);
     C.d = ChainDesc{};
     C.d.N = N; C.d.Lx = p.Nlx; C.d.Ly = p.Nly; C.d.Ltrot = p.Ltrot; C.d.Nwrap = p.Nwrap;
@@ -426,7 +439,7 @@ extern "C" int z2_create(z2_handle **out, const z2_chain_params *params, int32_t
     const int N = C.N;
     size_t arena = (h->smem - smem_small_bytes(N)) / 8;
     size_t nn = (size_t)N * C.d.ldg;
-    if (C.d.g_in_smem && nn + std::max<size_t>(2 * (size_t)z2_ldx(N) * C.d.k2, kGemmTile) > arena)
+    if (C.d.g_in_smem && nn + std::max<size_t>(2 * (size_t)z2_ldx(N) * C.d.k2, tile_min(N)) > arena)
       C.d.g_in_smem = 0;
   }
   CUDA_TRY(h, cudaFuncSetAttribute(z2_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -570,6 +583,7 @@ extern "C" int z2_create(z2_handle **out, const z2_chain_params *params, int32_t
       d.ptime = std::max(0.0, std::min(1.0, pt));
     }
     d.hzero = std::fabs(p.h) <= kZero ? 1 : 0;
+    d.stab_exact = h->opt.stab_exact ? 1 : 0;
     d.kin_fused = kin_fused_size(lat);
     d.bonds = (const int *)(base + o_bonds); d.groups = (const int *)(base + o_groups);
     d.bbonds = (const int *)(base + o_bb); d.plaq = (const int *)(base + o_plaq);
@@ -988,6 +1002,7 @@ extern "C" int z2_tune_delay(const z2_chain_params *params, int32_t nchains,
     z2_options o{};
     o.delay_k = k;
     o.device = opt ? opt->device : 0;
+    o.stab_exact = opt ? opt->stab_exact : 0;
     z2_handle *h = nullptr;
     int rc = z2_create(&h, probe.data(), (int)probe.size(), &o);
     if (rc == Z2_OK) rc = z2_pre(h);

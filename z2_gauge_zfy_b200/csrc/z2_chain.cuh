@@ -1003,6 +1003,23 @@ __device__ __noinline__ void record_drift(const ChainDesc &c, double dif, bool s
   }
 }
 
+// The chain's stabilization: the reference's pivoted QR, or the pre-pivoted
+// blocked QR (dev_stab_U_fast / dev_stab_green_fast).
+__device__ __forceinline__ void chain_stab_U(const ChainDesc &c, const Smem &s, double *A, int lda,
+                                             double *U, double *D, double *V, bool left) {
+  if (c.stab_exact) dev_stab_U(s, c.N, A, lda, U, D, V, c.W0, left);
+  else dev_stab_U_fast(s, c.N, A, lda, U, D, V, c.W0, left);
+}
+__device__ __forceinline__ void chain_stab_green(const ChainDesc &c, const Smem &s, int nt, double *A,
+                                                 int lda, double *Gout) {
+  if (c.stab_exact)
+    dev_stab_green(s, c.N, nt, c.Ltrot, c.UR, c.DR, c.VR, c.ULT, c.DL, c.VL, A, lda, c.W1, c.W2,
+                   c.W0, Gout);
+  else
+    dev_stab_green_fast(s, c.N, nt, c.Ltrot, c.UR, c.DR, c.VR, c.ULT, c.DL, c.VL, A, lda, c.W1,
+                        c.W2, c.W0, Gout);
+}
+
 // Wrap_pre (src/stabilization.f90:374-398)
 __device__ __noinline__ void wrap_pre(const ChainDesc &c, const Smem &s, int nt, Pend &pd) {
   const int N = c.N, NN = N * N;
@@ -1011,7 +1028,7 @@ __device__ __noinline__ void wrap_pre(const ChainDesc &c, const Smem &s, int nt,
   if (nt != 0) {
     blk_copy(A, lda, c.UR, N, N, N);
     { PhTimer t(c, PH_PEND); apply_pending_R(c, s, A, lda, pd.lo, pd.hi, c.use_kin != 0); }
-    dev_stab_U(s, N, A, lda, c.UR, c.DR, c.VR, c.W0, false);
+    chain_stab_U(c, s, A, lda, c.UR, c.DR, c.VR, false);
   }
   pd.lo = 1; pd.hi = 0;
   { PhTimer t(c, PH_STACK);
@@ -1019,8 +1036,7 @@ __device__ __noinline__ void wrap_pre(const ChainDesc &c, const Smem &s, int nt,
     blk_copy(c.VRs + (size_t)st * NN, N, c.VR, N, N, N);
     copy_vec(c.DRs + (size_t)st * N, c.DR, N); }
   if (nt == c.Ltrot) {
-    dev_stab_green(s, N, nt, c.Ltrot, c.UR, c.DR, c.VR, c.ULT, c.DL, c.VL, A, lda, c.W1, c.W2,
-                   c.W0, c.G);
+    chain_stab_green(c, s, nt, A, lda, c.G);
   }
 }
 
@@ -1043,10 +1059,8 @@ __device__ __noinline__ void wrap_L(const ChainDesc &c, const Smem &s, int nt, P
   }
   pd.lo = 1; pd.hi = 0;
   if (nt != c.Ltrot) {
-    { PhTimer t(c, PH_STABU); dev_stab_U(s, N, A, lda, c.ULT, c.DL, c.VL, c.W0, true); }
-    { PhTimer t(c, PH_STABG);
-      dev_stab_green(s, N, nt, c.Ltrot, c.UR, c.DR, c.VR, c.ULT, c.DL, c.VL, A, lda, c.W1, c.W2,
-                     c.W0, c.W3); }
+    { PhTimer t(c, PH_STABU); chain_stab_U(c, s, A, lda, c.ULT, c.DL, c.VL, true); }
+    { PhTimer t(c, PH_STABG); chain_stab_green(c, s, nt, A, lda, c.W3); }
     double dif = blk_maxdiff(c.W3, N, c.G, N, N, s.red);
     record_drift(c, dif, stats);
     blk_copy(c.G, N, c.W3, N, N, N);
@@ -1077,10 +1091,8 @@ __device__ __noinline__ void wrap_R(const ChainDesc &c, const Smem &s, int nt, P
   }
   pd.lo = 1; pd.hi = 0;
   if (nt != 0) {
-    { PhTimer t(c, PH_STABU); dev_stab_U(s, N, A, lda, c.UR, c.DR, c.VR, c.W0, false); }
-    { PhTimer t(c, PH_STABG);
-      dev_stab_green(s, N, nt, c.Ltrot, c.UR, c.DR, c.VR, c.ULT, c.DL, c.VL, A, lda, c.W1, c.W2,
-                     c.W0, c.W3); }
+    { PhTimer t(c, PH_STABU); chain_stab_U(c, s, A, lda, c.UR, c.DR, c.VR, false); }
+    { PhTimer t(c, PH_STABG); chain_stab_green(c, s, nt, A, lda, c.W3); }
     double dif = blk_maxdiff(c.W3, N, c.G, N, N, s.red);
     record_drift(c, dif, stats);
     blk_copy(c.G, N, c.W3, N, N, N);

@@ -14,7 +14,7 @@ __device__ __noinline__ void wrap_tau(const ChainDesc &c, const Smem &s, int nt,
   blk_copy(A, lda, c.URd, N, N, N);
   apply_pending_R(c, s, A, lda, pd.lo, pd.hi, c.use_kin != 0);
   pd.lo = 1; pd.hi = 0;
-  dev_stab_U(s, N, A, lda, c.URd, c.DRd, c.VRd, c.W0, false);
+  chain_stab_U(c, s, A, lda, c.URd, c.DRd, c.VRd, false);
   dev_stab_green_big(s, N, c.URd, c.DRd, c.VRd, c.ULTd, c.DLd, c.VLd, c.W0, c.W1, c.W2, c.W3,
                      c.B0, c.B1, c.B2, c.B3);
   const double *T = c.B3;

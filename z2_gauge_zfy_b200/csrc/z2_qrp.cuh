@@ -387,6 +387,118 @@ __device__ __noinline__ void qrp_reg(double *A, int lda, int n, int *jpvt, doubl
   for (int l = tid; l < n; l += Z2_NT) jpvt[l] = lp2c[l] + 1;
   __syncthreads();
 }
+// Householder QR WITHOUT pivoting (DGEQR2 semantics) in the same register
+// tile, for the pre-pivoted stabilization: the columns are already in
+// decreasing norm order, so step j factors column j.  With no norm downdate
+// and no arg-max, a step has one block barrier: the reflector of column j
+// (its warp publishes v, tau) -> barrier -> every warp applies H_j to its
+// trailing columns.  v and tau alternate between two buffers by the parity
+// of j: the warp that writes the buffer of step j + 2 has passed the barrier
+// of step j + 1, which every reader of step j reaches only after its reads.
+// work: >= 2 n doubles; red: >= 32 doubles.
+template <int S>
+__device__ __noinline__ void qr_reg(double *A, int lda, int n, double *tau, double *work,
+                                    double *red) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tr = lane & 15, tc = (warp << 1) | (lane >> 4);
+  const int hl = lane & 16;
+  double *tsh = red + 24;                              // [2] tau of the step
+  double a[S][S];
+#pragma unroll
+  for (int p = 0; p < S; ++p)
+#pragma unroll
+    for (int q = 0; q < S; ++q) {
+      const int r = tr + 16 * p, c = tc + 16 * q;
+      a[p][q] = (r < n && c < n) ? A[r + (size_t)c * lda] : 0.0;
+    }
+  unsigned done = 0;   // bit q: column tc + 16 q factored (or outside the matrix)
+#pragma unroll
+  for (int q = 0; q < S; ++q)
+    if (tc + 16 * q >= n) done |= 1u << q;
+  for (int j = 0; j < n; ++j) {
+    const int qc = j >> 4, gc = j & 15;
+    const int pj = j >> 4, oj = j & 15;
+    double *vsh = work + (j & 1) * n;
+    // ---- reflector of column j (DLARFG), by the warp holding it; the
+    // finished column goes straight to A(:, j) ----
+    if (warp == (gc >> 1)) {
+      const bool mine = (lane >> 4) == (gc & 1);
+      double col[S];
+#pragma unroll
+      for (int p = 0; p < S; ++p) col[p] = 0.0;
+      switch (qc) {
+        QRP_CASE_COL(0) QRP_CASE_COL(1) QRP_CASE_COL(2) QRP_CASE_COL(3) QRP_CASE_COL(4)
+        QRP_CASE_COL(5) QRP_CASE_COL(6) QRP_CASE_COL(7) QRP_CASE_COL(8)
+        default: break;
+      }
+      double s0 = 0.0, s1 = 0.0, aj = 0.0;
+#pragma unroll
+      for (int p = 0; p < S; ++p) {
+        const int r = tr + 16 * p;
+        const double x = (r > j && r < n) ? col[p] : 0.0;
+        if (p & 1) s1 += x * x; else s0 += x * x;
+        if (p == pj) aj = col[p];
+      }
+      const double ss = hw_sum(s0 + s1);
+      const double alpha = __shfl_sync(Z2_FULL, aj, hl | oj);
+      double t = 0.0, beta = alpha, sc = 1.0;
+      if (j < n - 1 && ss != 0.0) {
+        double nb = sqrt(fma(alpha, alpha, ss));
+        if (isinf(nb)) nb = dlapy2(alpha, sqrt(ss));
+        beta = -copysign(nb, alpha);
+        t = (beta - alpha) / beta;
+        sc = 1.0 / (alpha - beta);
+      }
+      if (mine) {
+#pragma unroll
+        for (int p = 0; p < S; ++p) {
+          const int r = tr + 16 * p;
+          double vv = 0.0, out = col[p];
+          if (r > j) {
+            if (t != 0.0) out *= sc;
+            vv = out;
+          } else if (r == j) {
+            out = beta;
+            vv = 1.0;
+          }
+          if (r < n) {
+            vsh[r] = vv;
+            A[r + (size_t)j * lda] = out;
+          }
+        }
+        if (tr == 0) { tsh[j & 1] = t; tau[j] = t; }
+      }
+    }
+    __syncthreads();
+    if (tc == gc) done |= 1u << qc;
+    // ---- apply H_j to the trailing columns (DLARF) ----
+    const double t = tsh[j & 1];
+    if (t != 0.0) {
+      double vr[S], d[S];
+#pragma unroll
+      for (int p = 0; p < S; ++p) {
+        const int r = tr + 16 * p;
+        vr[p] = (r < n) ? vsh[r] : 0.0;   // 0 above row j
+        d[p] = 0.0;
+      }
+      switch (pj) {
+        QRP_CASE_DOT(0) QRP_CASE_DOT(1) QRP_CASE_DOT(2) QRP_CASE_DOT(3) QRP_CASE_DOT(4)
+        QRP_CASE_DOT(5) QRP_CASE_DOT(6) QRP_CASE_DOT(7) QRP_CASE_DOT(8)
+        default: break;
+      }
+      qrp_colsum<S>(d, tr, hl);
+#pragma unroll
+      for (int q = 0; q < S; ++q) d[q] = ((done >> q) & 1u) ? 0.0 : t * d[q];
+      switch (pj) {
+        QRP_CASE_UPD(0) QRP_CASE_UPD(1) QRP_CASE_UPD(2) QRP_CASE_UPD(3) QRP_CASE_UPD(4)
+        QRP_CASE_UPD(5) QRP_CASE_UPD(6) QRP_CASE_UPD(7) QRP_CASE_UPD(8)
+        default: break;
+      }
+    }
+  }
+  __syncthreads();
+}
+
 #undef QRP_CASE_COL
 #undef QRP_CASE_ROW
 #undef QRP_CASE_DOT
@@ -412,4 +524,23 @@ __device__ __forceinline__ void blk_geqp3_fast(double *A, int lda, int n, int *j
     }
   }
   blk_geqp3_tc(A, lda, n, jpvt, tau, vn1, vn2);
+}
+
+// QR without pivoting of the pre-pivoted stabilization, register-resident for
+// n <= 144 (false when the size or the work space does not allow it).
+__device__ __forceinline__ bool qr_reg_any(double *A, int lda, int n, double *tau, double *work,
+                                           int wd, double *red) {
+  if (work == nullptr || wd < 2 * n) return false;
+  switch ((n + 15) >> 4) {
+    case 1: qr_reg<1>(A, lda, n, tau, work, red); return true;
+    case 2: qr_reg<2>(A, lda, n, tau, work, red); return true;
+    case 3: qr_reg<3>(A, lda, n, tau, work, red); return true;
+    case 4: qr_reg<4>(A, lda, n, tau, work, red); return true;
+    case 5: qr_reg<5>(A, lda, n, tau, work, red); return true;
+    case 6: qr_reg<6>(A, lda, n, tau, work, red); return true;
+    case 7: qr_reg<7>(A, lda, n, tau, work, red); return true;
+    case 8: qr_reg<8>(A, lda, n, tau, work, red); return true;
+    case 9: qr_reg<9>(A, lda, n, tau, work, red); return true;
+    default: return false;
+  }
 }
