@@ -232,11 +232,11 @@ def _cpu_cost(c) -> float:
     return c.Ltrot * n * n * (92.0 + 0.8 * n + 14.0 * n / c.Nwrap)
 
 
-def parity_and_cpu_baseline(device: int, kmap: dict) -> tuple[dict, dict]:
+def parity_and_cpu_baseline(device: int, kmap: dict, smap: dict) -> tuple[dict, dict]:
     """The metric's accuracy condition, checked on the benched configuration:
     one chain of each of the 12 (L, beta) classes of the batched workload plus
     the single-chain configuration, one bin each in ONE batched launch with
-    the tuned delay ranks, against the C restatement of the reference path
+    the tuned delay ranks and flush shapes, against the C restatement of the reference path
     (oracle/c/z2cpu.c, reference LAPACK, 1 thread) from the same seeds.  The
     C restatement's bin times of the 12 batched classes are the 1-core CPU
     baseline.  Returns (parity, cpu_baseline)."""
@@ -244,7 +244,8 @@ def parity_and_cpu_baseline(device: int, kmap: dict) -> tuple[dict, dict]:
     from z2_gauge_zfy_b200 import Z2Batch
     chains = batched_chains()[:12] + single_chain()
     ks = [int(kmap.get(c.N, 0)) for c in chains]
-    with Z2Batch(chains, device=device, record=True, delay_k_chain=ks) as b:
+    ss = [int(smap.get(c.N, 0)) for c in chains]
+    with Z2Batch(chains, device=device, record=True, delay_k_chain=ks, flush_shape_chain=ss) as b:
         b.pre()
         b.sweep(1, False)
         gpu = [(b.green(i), b.obs_equal(i), b.stats(i)["Xmaxm"], b.decisions(i)[0],
@@ -407,17 +408,17 @@ def main():
         __graft_entry__.build()
     if dist is not None:
         dist.barrier()
-    from z2_gauge_zfy_b200 import Z2Batch, load, tune_delay
+    from z2_gauge_zfy_b200 import FLUSH_SHAPES, Z2Batch, load, tune
     load()
 
     chains = batched_chains(rank, args.chains)
     su_step = site_updates(chains)
-    # delayed-update rank per lattice size from the library's autotuner
-    # (short probe chains, before the timed region)
+    # delayed-update rank and flush tile shape per lattice size from the
+    # library's autotuner (short probe chains, before the timed region)
     t_tune = time.perf_counter()
-    kchain = tune_delay(chains, local)
+    kchain, schain = tune(chains, local)
     t_tune = time.perf_counter() - t_tune
-    b = Z2Batch(chains, device=local, delay_k_chain=kchain)
+    b = Z2Batch(chains, device=local, delay_k_chain=kchain, flush_shape_chain=schain)
     b.pre()
     for _ in range(args.warmup):
         b.sweep(1, False)
@@ -474,6 +475,7 @@ def main():
     peak = fp64_peak_tflops(local)
     achieved = flops_launch / launch_s / 1e12
     kmap = {c.N: int(k) for c, k in zip(chains, kchain)}
+    smap = {c.N: int(x) for c, x in zip(chains, schain)}
     line = {
         "metric": "spacetime site-updates/s", "value": value, "unit": "site-updates/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -484,6 +486,10 @@ def main():
         "parallelism": f"chains sharded over {world} GPU(s), replicas",
         "accept_rate": a_rate,
         "delay_rank": ",".join(f"N{n}:k{k}" for n, k in sorted(kmap.items())),
+        "flush_shape": ",".join(f"N{n}:{FLUSH_SHAPES[x]}" for n, x in sorted(smap.items())),
+        "tuning": "z2_tune: ranks 4..64 (shared memory caps them: k <= 8 at N = 144) x every "
+                  "flush tile shape valid for N, median SM cycles of 3 probe chains, first "
+                  "within 1.5 % of the fastest in the order (default shape, smaller rank)",
         "autotune_s": t_tune,
         "bin_observables_mean": dict(zip(("flux_avg", "chi_flux", "pair_sc_q0", "cdw_pi",
                                           "cdw_shift", "cdw_ratio", "density"),
@@ -516,7 +522,7 @@ def main():
         line["adjoint"] = adjoint_cost(local)
         line["large_batched"] = large_batched(local)
     if rank == 0:
-        parity, base = parity_and_cpu_baseline(local, kmap)
+        parity, base = parity_and_cpu_baseline(local, kmap, smap)
         line["parity"] = parity
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = base

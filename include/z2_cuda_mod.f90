@@ -18,7 +18,8 @@ module z2_cuda_mod
     end type
     type, bind(C) :: z2_options
         integer(c_int32_t) :: delay_k, record, device, tau, graph
-        type(c_ptr)     :: delay_k_chain    ! c_null_ptr, or c_loc(k(1)) from z2_tune_delay
+        type(c_ptr)     :: delay_k_chain    ! c_null_ptr, or c_loc(k(1)) from z2_tune
+        type(c_ptr)     :: flush_shape_chain ! c_null_ptr, or c_loc(s(1)) from z2_tune
         integer(c_int32_t) :: stab_exact    ! 1 = the reference's pivoted QR in the wraps
     end type
     interface
@@ -73,6 +74,10 @@ module z2_cuda_mod
         integer(c_int) function z2_tune_delay(p, n, opt, k) bind(C, name="z2_tune_delay")
             import; type(z2_chain_params) :: p(*); integer(c_int32_t), value :: n
             type(z2_options) :: opt; integer(c_int32_t) :: k(*)
+        end function
+        integer(c_int) function z2_tune(p, n, opt, k, shape) bind(C, name="z2_tune")
+            import; type(z2_chain_params) :: p(*); integer(c_int32_t), value :: n
+            type(z2_options) :: opt; integer(c_int32_t) :: k(*), shape(*)
         end function
         integer(c_int) function z2_stab_green(h, chain, UR, DR, VR, UL, DL, VL, nt, G) &
                 bind(C, name="z2_stab_green")

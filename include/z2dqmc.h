@@ -76,6 +76,12 @@ typedef struct z2_options {
   int32_t tau;       /* 1: allocate the time-displaced chain (is_tau) */
   int32_t graph;     /* 1: capture each bin's launch as a CUDA graph, replayed */
   const int32_t *delay_k_chain;  /* optional [nchains] per-chain delay rank (autotuner) */
+  const int32_t *flush_shape_chain;  /* optional [nchains] tile shape of each chain's
+                          rank-2k flush (z2_tune picks it; 0 = by divisibility):
+                          1 bounded 16x16 groups, 2 bounded 8x8 groups, 3 8x8
+                          blocks (8 | N), 4 16x16 (16 | N), 5 24x24 (24 | N),
+                          6 16x8 (16 | N), 7 24x16 (48 | N).  All shapes give
+                          the same bits. */
   int32_t stab_exact;  /* 1: stabilize with the reference's column-pivoted QR
                           (ZGEQP3) and its stab_green branches; 0: pre-pivoted
                           blocked QR and the scale-split Green's function (the
@@ -177,6 +183,18 @@ int z2_get_global_stats(const z2_handle *h, int32_t chain, double out[5]);
  * allocates and frees its own probe handles. */
 int z2_tune_delay(const z2_chain_params *params, int32_t nchains, const z2_options *opt,
                   int32_t *k_out);
+/* Joint autotuner of the delayed-update rank and the flush tile shape (no
+ * reference counterpart).  For every distinct lattice size it times one bin of
+ * three short probe chains per candidate (the chain's couplings and time step,
+ * Ltrot cut to 2*Nwrap; ranks 4..64 as z2_tune_delay, capped by shared memory,
+ * times every flush shape valid for N) by the SM cycles of the chain kernel,
+ * takes the median over the three probes, and picks, in the order (default
+ * shape first, then smaller rank), the first candidate within 1.5 % of the
+ * fastest, so that repeated runs pick the same configuration.  k_out and
+ * shape_out [nchains] are ready to pass as z2_options.delay_k_chain and
+ * flush_shape_chain. */
+int z2_tune(const z2_chain_params *params, int32_t nchains, const z2_options *opt,
+            int32_t *k_out, int32_t *shape_out);
 /* The first n recorded decisions and ratios of one chain; dec and ratios are
  * each optional. */
 int z2_get_decisions(const z2_handle *h, int32_t chain, uint8_t *dec,

@@ -4,7 +4,8 @@ One chain of each of the 12 (L, beta) classes of the batched workload
 (L in {6, 8, 10, 12}, beta in {8, 12, 16} at dtau 0.1, h ~ U[0.2, 1], K = 0.5,
 Nwrap 10) plus the single-chain plain configuration (L = 8, beta = 10, 100
 slices) run side by side in ONE batched launch, with the delayed-update
-ranks the library's autotuner picks, exactly as bench.py builds them.  Each
+ranks and flush tile shapes the library's autotuner picks, exactly as
+bench.py builds them.  Each
 chain is compared over a whole bin (Local_sweep with Nsweep = 1:
 src/local_sweep.f90:152-195; flips src/localK.f90:45-173; stabilization
 src/stabilization.f90:122-200, 400-476) with the C restatement of the
@@ -25,7 +26,7 @@ import pytest
 
 from bench import batched_chains, single_chain
 from oracle import z2cpu
-from z2_gauge_zfy_b200 import Z2Batch, tune_delay
+from z2_gauge_zfy_b200 import Z2Batch, tune
 
 pytestmark = pytest.mark.gpu
 RTOL = 1e-10
@@ -43,8 +44,9 @@ def test_bench_classes_whole_bin_match_c_port(stab_exact):
     chains = batched_chains()[:12] + single_chain()
     assert sorted({(c.Nlx, c.Ltrot) for c in chains[:12]}) == \
         [(L, Lt) for L in (6, 8, 10, 12) for Lt in (80, 120, 160)]
-    k = tune_delay(chains, stab_exact=stab_exact)
-    with Z2Batch(chains, record=True, delay_k_chain=k, stab_exact=stab_exact) as b:
+    k, shape = tune(chains, stab_exact=stab_exact)
+    with Z2Batch(chains, record=True, delay_k_chain=k, flush_shape_chain=shape,
+                 stab_exact=stab_exact) as b:
         b.pre()
         b.sweep(1, False)
         gpu = [dict(G=b.green(i), obs=b.obs_equal(i), st=b.stats(i), dec=b.decisions(i)[0],
@@ -57,7 +59,7 @@ def test_bench_classes_whole_bin_match_c_port(stab_exact):
         st = c.state()
         c.close()
         g = gpu[i]
-        tag = f"chain {i} (L={ch.Nlx}, Ltrot={ch.Ltrot}, k={k[i]})"
+        tag = f"chain {i} (L={ch.Nlx}, Ltrot={ch.Ltrot}, k={k[i]}, shape={shape[i]})"
         assert np.array_equal(g["dec"], dec), tag
         sig, iseed = g["cfg"]
         assert np.array_equal(sig, st["sigma"]), tag

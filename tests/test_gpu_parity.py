@@ -323,3 +323,43 @@ def test_delay_autotuner():
     for (g0, d0), (g1, d1) in zip(*outs):
         assert np.array_equal(d0, d1)
         assert rel(g1, g0) < RTOL
+
+
+def test_flush_shapes_identical_bits():
+    """Every tile shape of the rank-2k flush forms each element of G with the
+    same k chunks, so a batch run with any valid shape makes the same
+    decisions and leaves the same G, to the bit (N = 144 admits all seven
+    explicit shapes, N = 64 four, N = 36 the two bounded ones)."""
+    from z2_gauge_zfy_b200 import FLUSH_SHAPES
+    chains = [Chain(RT=1.0, J=0.5, h=0.6, Nlx=L, Nly=L, Ltrot=20, beta=2.0, Nwrap=10, seed=70 + L)
+              for L in (12, 8, 6)]
+    ok = {144: set(range(8)), 64: {0, 1, 2, 3, 4, 6}, 36: {0, 1, 2}}
+    ref = None
+    for shape in sorted(FLUSH_SHAPES):
+        sh = [shape if shape in ok[c.N] else 0 for c in chains]
+        with Z2Batch(chains, record=True, delay_k=8, flush_shape_chain=sh) as b:
+            b.pre()
+            b.sweep(1, False)
+            out = [(b.green(i), b.decisions(i)[0]) for i in range(len(chains))]
+        if ref is None:
+            ref = out
+            continue
+        for (g0, d0), (g1, d1) in zip(ref, out):
+            assert np.array_equal(d0, d1), shape
+            assert np.array_equal(g0, g1), shape
+
+
+def test_tuner_shapes_valid_and_repeatable():
+    """z2_tune picks one (rank, shape) per lattice size, valid for that size,
+    and two consecutive calls pick the same."""
+    from z2_gauge_zfy_b200 import tune
+    chains = [Chain(RT=1.0, J=0.5, h=0.5, Nlx=L, Nly=L, Ltrot=40, beta=4.0, Nwrap=10, seed=s)
+              for L, s in ((6, 1), (8, 2), (12, 3), (6, 4), (12, 5))]
+    k1, s1 = tune(chains)
+    k2, s2 = tune(chains)
+    assert np.array_equal(k1, k2) and np.array_equal(s1, s2), (k1, s1, k2, s2)
+    assert k1[0] == k1[3] and s1[0] == s1[3] and k1[2] == k1[4] and s1[2] == s1[4]
+    ok = {36: {0, 1, 2}, 64: {0, 1, 2, 3, 4, 6}, 144: set(range(8))}
+    for c, k, s in zip(chains, k1, s1):
+        assert int(s) in ok[c.N], (c.N, s)
+        assert k in (4, 6, 8, 12, 16, 24, 32, 48, 64)

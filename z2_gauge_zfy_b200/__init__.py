@@ -8,8 +8,8 @@ The compute lives in the in-tree CUDA library ``libz2dqmc.so`` behind the C
 ABI of ``include/z2dqmc.h``; this package is its host-side binding.
 """
 from ._ffi import LIB_PATH, Z2Error, load  # noqa: F401
-from .api import (OBS_EQ_NAMES, OBS_TAU_NAMES, STAT_NAMES, Chain,  # noqa: F401
-                  Z2Batch, tune_delay)
+from .api import (FLUSH_SHAPES, OBS_EQ_NAMES, OBS_TAU_NAMES, STAT_NAMES,  # noqa: F401
+                  Chain, Z2Batch, tune, tune_delay)
 
 __all__ = ["Chain", "Z2Batch", "Z2Error", "load", "LIB_PATH", "OBS_EQ_NAMES",
-           "OBS_TAU_NAMES", "STAT_NAMES", "tune_delay"]
+           "OBS_TAU_NAMES", "STAT_NAMES", "tune", "tune_delay", "FLUSH_SHAPES"]

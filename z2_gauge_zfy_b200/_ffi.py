@@ -35,7 +35,7 @@ EXPORTS = (
     "z2_propT_R", "z2_propgrT_R", "z2_wrap_pre", "z2_wrap_L", "z2_wrap_R", "z2_wrap_tau",
     "z2_dyn_reset", "z2_prop_slice_L", "z2_prop_slice_R", "z2_sweep_reset",
     "z2_obs_equal_calc", "z2_obs_equal_ave", "z2_obs_tau_calc", "z2_obs_tau_ave",
-    "z2_get_prop", "z2_set_prop", "z2_get_propgr",
+    "z2_get_prop", "z2_set_prop", "z2_get_propgr", "z2_tune",
 )
 # entry points (handle, chain, nt) and (handle, chain) of the state mirrors
 STATE_NT = ("z2_propK_pre", "z2_propK_L", "z2_propK_R", "z2_propgrK_R", "z2_wrap_pre",
@@ -66,7 +66,8 @@ class Options(C.Structure):
     """``z2_options``."""
     _fields_ = [("delay_k", C.c_int32), ("record", C.c_int32), ("device", C.c_int32),
                 ("tau", C.c_int32), ("graph", C.c_int32),
-                ("delay_k_chain", C.POINTER(C.c_int32)), ("stab_exact", C.c_int32)]
+                ("delay_k_chain", C.POINTER(C.c_int32)),
+                ("flush_shape_chain", C.POINTER(C.c_int32)), ("stab_exact", C.c_int32)]
 
 
 _lib = None
@@ -113,6 +114,8 @@ def load():
         "z2_get_global_stats": (C.c_int, [vp, i32, dp]),
         "z2_tune_delay": (C.c_int, [C.POINTER(ChainParams), i32, C.POINTER(Options),
                                    C.POINTER(i32)]),
+        "z2_tune": (C.c_int, [C.POINTER(ChainParams), i32, C.POINTER(Options), C.POINTER(i32),
+                             C.POINTER(i32)]),
         "z2_wrap_L": (C.c_int, [vp, i32, i32, i32]),
         "z2_wrap_R": (C.c_int, [vp, i32, i32, i32]),
         "z2_sweep_reset": (C.c_int, [vp, i32, i32]),

@@ -107,7 +107,7 @@ def tune_delay(chains, device: int = 0, stab_exact: bool = False) -> np.ndarray:
     lib = _ffi.load()
     chains = list(chains)
     arr, _keep = _params(chains)
-    opt = Options(0, 0, device, 0, 0, None, 1 if stab_exact else 0)
+    opt = Options(0, 0, device, 0, 0, None, None, 1 if stab_exact else 0)
     k = np.zeros(len(chains), dtype=np.int32)
     code = lib.z2_tune_delay(arr, len(chains), C.byref(opt),
                              k.ctypes.data_as(C.POINTER(C.c_int32)))
@@ -116,23 +116,44 @@ def tune_delay(chains, device: int = 0, stab_exact: bool = False) -> np.ndarray:
     return k
 
 
+FLUSH_SHAPES = {0: "by divisibility", 1: "bounded 16x16", 2: "bounded 8x8", 3: "8x8 blocks",
+                4: "16x16 blocks", 5: "24x24 blocks", 6: "16x8 blocks", 7: "24x16 blocks"}
+
+
+def tune(chains, device: int = 0, stab_exact: bool = False):
+    """Per-chain delayed-update rank and flush tile shape picked jointly by the
+    library's autotuner (``z2_tune``): returns (k, shape), int32 arrays."""
+    lib = _ffi.load()
+    chains = list(chains)
+    arr, _keep = _params(chains)
+    opt = Options(0, 0, device, 0, 0, None, None, 1 if stab_exact else 0)
+    k = np.zeros(len(chains), dtype=np.int32)
+    sh = np.zeros(len(chains), dtype=np.int32)
+    code = lib.z2_tune(arr, len(chains), C.byref(opt), k.ctypes.data_as(C.POINTER(C.c_int32)),
+                       sh.ctypes.data_as(C.POINTER(C.c_int32)))
+    if code != 0:
+        raise Z2Error(code, "z2_tune failed")
+    return k, sh
+
+
 class Z2Batch:
     """A batch of chains resident on one GPU (``z2_create``)."""
 
     def __init__(self, chains, delay_k=0, record: bool = False, device: int = 0,
                  tau: bool = False, graph: bool = False, delay_k_chain=None,
-                 stab_exact: bool = False):
+                 stab_exact: bool = False, flush_shape_chain=None):
         """delay_k: rank of the delayed updates for every chain (0 = built-in
         default per lattice size), or "auto" to run the autotuner
-        (``z2_tune_delay``) and use its per-chain ranks.  stab_exact: stabilize
-        with the reference's column-pivoted QR instead of the pre-pivoted
-        blocked QR (``z2_options.stab_exact``)."""
+        (``z2_tune``) and use its per-chain ranks and flush tile shapes.
+        stab_exact: stabilize with the reference's column-pivoted QR instead of
+        the pre-pivoted QR (``z2_options.stab_exact``).  flush_shape_chain:
+        per-chain tile shape of the rank-2k flush (``FLUSH_SHAPES``)."""
         self.lib = _ffi.load()
         self.chains = list(chains)
         n = len(self.chains)
         arr, self._rt_keep = _params(self.chains)
         if delay_k == "auto":
-            delay_k_chain = tune_delay(self.chains, device, stab_exact)
+            delay_k_chain, flush_shape_chain = tune(self.chains, device, stab_exact)
             delay_k = 0
         self._kc = None
         kc_ptr = None
@@ -142,8 +163,16 @@ class Z2Batch:
                 raise Z2Error(1, f"delay_k_chain has shape {self._kc.shape}, "
                                  f"needs one rank per chain ({n},)")
             kc_ptr = self._kc.ctypes.data_as(C.POINTER(C.c_int32))
+        self._fs = None
+        fs_ptr = None
+        if flush_shape_chain is not None:
+            self._fs = np.ascontiguousarray(flush_shape_chain, dtype=np.int32)
+            if self._fs.shape != (n,):
+                raise Z2Error(1, f"flush_shape_chain has shape {self._fs.shape}, "
+                                 f"needs one shape per chain ({n},)")
+            fs_ptr = self._fs.ctypes.data_as(C.POINTER(C.c_int32))
         opt = Options(delay_k, 1 if record else 0, device, 1 if tau else 0, 1 if graph else 0,
-                      kc_ptr, 1 if stab_exact else 0)
+                      kc_ptr, fs_ptr, 1 if stab_exact else 0)
         h = C.c_void_p()
         code = self.lib.z2_create(C.byref(h), arr, n, C.byref(opt))
         self.h = h

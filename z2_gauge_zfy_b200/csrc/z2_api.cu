@@ -368,6 +368,9 @@ extern "C" int z2_create(z2_handle **out, const z2_chain_params *params, int32_t
     if (!(p.beta > 0.0)) return set_err(h, Z2_ERR_ARG, "chain %d: beta must be positive", c);
     if (p.Nlx * p.Nly > 1024)
       return set_err(h, Z2_ERR_ARG, "chain %d: N = %d exceeds 1024", c, p.Nlx * p.Nly);
+    if (h->opt.flush_shape_chain && !flush_shape_ok(h->opt.flush_shape_chain[c], p.Nlx * p.Nly))
+      return set_err(h, Z2_ERR_ARG, "chain %d: flush shape %d does not fit N = %d", c,
+                     h->opt.flush_shape_chain[c], p.Nlx * p.Nly);
   }
   CUDA_TRY(h, cudaSetDevice(h->device));
   // ranf multiplier powers
@@ -584,6 +587,7 @@ extern "C" int z2_create(z2_handle **out, const z2_chain_params *params, int32_t
     }
     d.hzero = std::fabs(p.h) <= kZero ? 1 : 0;
     d.stab_exact = h->opt.stab_exact ? 1 : 0;
+    d.flush_shape = h->opt.flush_shape_chain ? h->opt.flush_shape_chain[c] : 0;
     d.kin_fused = kin_fused_size(lat);
     d.bonds = (const int *)(base + o_bonds); d.groups = (const int *)(base + o_groups);
     d.bbonds = (const int *)(base + o_bb); d.plaq = (const int *)(base + o_plaq);
@@ -958,22 +962,49 @@ extern "C" int z2_get_phase_cycles(const z2_handle *h, int32_t chain, double out
 }
 
 // ---------------------------------------------------------------------------
-// Delay-rank autotuner.  The reference applies every accepted flip to G at
-// once (src/localK.f90:141-165); here flips are queued and flushed as one
-// rank-2k GEMM, and the best k trades the flush GEMM's efficiency (grows with
-// k) against the per-proposal corrections and the column build (grow with
-// k).  For each distinct lattice size the tuner runs short probe chains with
-// the chain's own couplings and time step (Ltrot cut to 2 Nwrap) at every
-// candidate rank, all sizes side by side in one persistent launch per
-// candidate, and keeps the rank with the fewest SM cycles per bin.
+// Autotuner of the delay rank and the flush tile shape.  The reference applies
+// every accepted flip to G at once (src/localK.f90:141-165); here flips are
+// queued and flushed as one rank-2k GEMM, and the best k trades the flush
+// GEMM's efficiency (grows with k) against the per-proposal corrections and
+// the column build (grow with k); the tile shape of the flush trades the load
+// balance of its N x N blocks over the 8 warps against fragment reuse.  Every
+// (k, shape) gives the same decisions, so the choice is a matter of time only.
 // ---------------------------------------------------------------------------
 static const int kTuneCand[] = {4, 6, 8, 12, 16, 24, 32, 48, 64};
+static const int kTuneShapes[] = {FS_DEFAULT, FS_GEN16, FS_GEN8, FS_T11, FS_T22, FS_T33, FS_T21,
+                                  FS_T32};
 
-extern "C" int z2_tune_delay(const z2_chain_params *params, int32_t nchains,
-                             const z2_options *opt, int32_t *k_out) {
+// SM cycles of one bin of every probe chain (after a warm-up bin), the
+// chain kernel's phases summed (flushes are nested in the proposals).
+static int probe_cycles(const std::vector<z2_chain_params> &probe, const z2_options &o,
+                        std::vector<double> &cyc) {
+  z2_handle *h = nullptr;
+  const int n = (int)probe.size();
+  int rc = z2_create(&h, probe.data(), n, &o);
+  if (rc == Z2_OK) rc = z2_pre(h);
+  if (rc == Z2_OK) rc = z2_sweep(h, 1, 0);
+  std::vector<double> c0((size_t)n * Z2_NPHASE), c1((size_t)n * Z2_NPHASE);
+  for (int c = 0; rc == Z2_OK && c < n; ++c) rc = z2_get_phase_cycles(h, c, &c0[(size_t)c * Z2_NPHASE]);
+  if (rc == Z2_OK) rc = z2_sweep(h, 1, 0);
+  for (int c = 0; rc == Z2_OK && c < n; ++c) rc = z2_get_phase_cycles(h, c, &c1[(size_t)c * Z2_NPHASE]);
+  cyc.assign(n, 0.0);
+  for (int c = 0; rc == Z2_OK && c < n; ++c)
+    for (int ph : {PH_KIN, PH_PROP, PH_OBS, PH_WRAP, PH_DYN})
+      cyc[c] += c1[(size_t)c * Z2_NPHASE + ph] - c0[(size_t)c * Z2_NPHASE + ph];
+  z2_destroy(h);
+  return rc;
+}
+
+// The delay rank (and, with shapes, the flush tile shape) per distinct
+// lattice size: three probe chains per size (the chain's couplings and time
+// step, Ltrot cut to 2 Nwrap), every size side by side in one launch per
+// candidate, the median SM cycles of the three, and the first candidate in
+// preference order (default shape, then smaller rank) within 1.5 % of the
+// fastest.
+static int tune_core(const z2_chain_params *params, int nchains, const z2_options *opt,
+                     bool shapes, int32_t *k_out, int32_t *shape_out) {
   if (!params || nchains <= 0 || !k_out) return Z2_ERR_ARG;
-  const int reps = 2;
-  // one representative chain per distinct N
+  const int reps = 3;
   std::vector<int> sizes, rep;
   for (int c = 0; c < nchains; ++c) {
     const int N = params[c].Nlx * params[c].Nly;
@@ -996,47 +1027,79 @@ extern "C" int z2_tune_delay(const z2_chain_params *params, int32_t nchains,
       probe.push_back(q);
     }
   }
-  std::vector<double> best(ns, 1e300);
-  std::vector<int> bestk(ns, 0), lastk(ns, -1);
+  z2_options base{};
+  base.device = opt ? opt->device : 0;
+  base.stab_exact = opt ? opt->stab_exact : 0;
+  // the ranks shared memory allows for each size (no launch: the plan only)
+  std::vector<std::vector<int>> ks(ns);
   for (int k : kTuneCand) {
-    z2_options o{};
+    z2_options o = base;
     o.delay_k = k;
-    o.device = opt ? opt->device : 0;
-    o.stab_exact = opt ? opt->stab_exact : 0;
     z2_handle *h = nullptr;
     int rc = z2_create(&h, probe.data(), (int)probe.size(), &o);
-    if (rc == Z2_OK) rc = z2_pre(h);
-    if (rc == Z2_OK) rc = z2_sweep(h, 1, 0);   // warm-up bin
-    std::vector<double> c0(probe.size() * Z2_NPHASE), c1(probe.size() * Z2_NPHASE);
-    for (int c = 0; rc == Z2_OK && c < (int)probe.size(); ++c)
-      rc = z2_get_phase_cycles(h, c, &c0[(size_t)c * Z2_NPHASE]);
-    if (rc == Z2_OK) rc = z2_sweep(h, 1, 0);
-    for (int c = 0; rc == Z2_OK && c < (int)probe.size(); ++c)
-      rc = z2_get_phase_cycles(h, c, &c1[(size_t)c * Z2_NPHASE]);
-    if (rc != Z2_OK) {
-      z2_destroy(h);
-      return rc;
-    }
+    if (rc != Z2_OK) { z2_destroy(h); return rc; }
     for (int i = 0; i < ns; ++i) {
-      // the rank actually used (shared memory may cap it)
-      const int keff = h->ch[i * reps].d.k2 / 2;
-      if (keff == lastk[i]) continue;
-      lastk[i] = keff;
-      double cyc = 0.0;
-      for (int r = 0; r < reps; ++r) {
-        const size_t b = (size_t)(i * reps + r) * Z2_NPHASE;
-        for (int ph : {PH_KIN, PH_PROP, PH_OBS, PH_WRAP, PH_DYN}) cyc += c1[b + ph] - c0[b + ph];
-      }
-      if (cyc < best[i]) { best[i] = cyc; bestk[i] = keff; }
+      const int keff = h->ch[(size_t)i * reps].d.k2 / 2;
+      if (std::find(ks[i].begin(), ks[i].end(), keff) == ks[i].end()) ks[i].push_back(keff);
     }
     z2_destroy(h);
+  }
+  struct Cand { int k, shape; };
+  std::vector<std::vector<Cand>> cands(ns);
+  size_t ncmax = 0;
+  for (int i = 0; i < ns; ++i) {
+    for (int sh : kTuneShapes) {
+      if (!shapes && sh != FS_DEFAULT) continue;
+      if (!flush_shape_ok(sh, sizes[i])) continue;
+      for (int k : ks[i]) cands[i].push_back({k, sh});
+    }
+    ncmax = std::max(ncmax, cands[i].size());
+  }
+  std::vector<std::vector<double>> cost(ns);
+  std::vector<int32_t> kc(probe.size()), sc(probe.size());
+  std::vector<double> cyc;
+  for (size_t ci = 0; ci < ncmax; ++ci) {
+    for (int i = 0; i < ns; ++i) {
+      const Cand &cd = cands[i][std::min(ci, cands[i].size() - 1)];
+      for (int r = 0; r < reps; ++r) { kc[(size_t)i * reps + r] = cd.k; sc[(size_t)i * reps + r] = cd.shape; }
+    }
+    z2_options o = base;
+    o.delay_k_chain = kc.data();
+    o.flush_shape_chain = sc.data();
+    const int rc = probe_cycles(probe, o, cyc);
+    if (rc != Z2_OK) return rc;
+    for (int i = 0; i < ns; ++i) {
+      if (ci >= cands[i].size()) continue;
+      double v[reps];
+      for (int r = 0; r < reps; ++r) v[r] = cyc[(size_t)i * reps + r];
+      std::sort(v, v + reps);
+      cost[i].push_back(v[reps / 2]);
+    }
+  }
+  std::vector<Cand> pick(ns);
+  for (int i = 0; i < ns; ++i) {
+    const double best = *std::min_element(cost[i].begin(), cost[i].end());
+    for (size_t ci = 0; ci < cands[i].size(); ++ci)
+      if (cost[i][ci] <= 1.015 * best) { pick[i] = cands[i][ci]; break; }
   }
   for (int c = 0; c < nchains; ++c) {
     const int N = params[c].Nlx * params[c].Nly;
     const int i = (int)(std::find(sizes.begin(), sizes.end(), N) - sizes.begin());
-    k_out[c] = bestk[i];
+    k_out[c] = pick[i].k;
+    if (shape_out) shape_out[c] = pick[i].shape;
   }
   return Z2_OK;
+}
+
+extern "C" int z2_tune_delay(const z2_chain_params *params, int32_t nchains,
+                             const z2_options *opt, int32_t *k_out) {
+  return tune_core(params, nchains, opt, false, k_out, nullptr);
+}
+
+extern "C" int z2_tune(const z2_chain_params *params, int32_t nchains, const z2_options *opt,
+                       int32_t *k_out, int32_t *shape_out) {
+  if (!shape_out) return Z2_ERR_ARG;
+  return tune_core(params, nchains, opt, true, k_out, shape_out);
 }
 
 static int upload_desc(z2_handle *h, int chain) {

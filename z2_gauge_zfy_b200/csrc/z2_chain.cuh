@@ -598,47 +598,50 @@ __device__ __noinline__ void flush_tiles(double *G, int ldg, const double *X, co
   __syncthreads();
 }
 
-// The same update for any N: 16 x 16 groups with bounds checks (the k loop
-// and epilogue of blk_dmma's general path).
+// The same update for any N: (8 GS) x (8 GS) groups with bounds checks (the k
+// loop and epilogue of blk_dmma's general path).
+template <int GS>
 __device__ __noinline__ void flush_generic(double *G, int ldg, const double *X, const double *Yt,
                                            int N, int ldx, int m) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int lr = lane >> 2, lc = lane & 3;
-  const int gm = (N + 15) >> 4;
+  const int gm = (N + 8 * GS - 1) / (8 * GS);
   for (int g = warp; g < gm * gm; g += Z2_WARPS) {
-    const int r0 = (g % gm) << 4, c0 = (g / gm) << 4;
-    const int ra0 = r0 + lr, ra1 = ra0 + 8, cb0 = c0 + lr, cb1 = cb0 + 8;
-    double acc[2][2][2];
+    const int r0 = (g % gm) * 8 * GS, c0 = (g / gm) * 8 * GS;
+    double acc[GS][GS][2];
 #pragma unroll
-    for (int a = 0; a < 2; ++a)
+    for (int a = 0; a < GS; ++a)
 #pragma unroll
-      for (int b = 0; b < 2; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+      for (int b = 0; b < GS; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
     for (int l0 = 0; l0 < m; l0 += 4) {
       const int l = l0 + lc;
       const bool lk = l < m;
-      const double a0 = (lk && ra0 < N) ? X[xy_at(ra0, l, ldx)] : 0.0;
-      const double a1 = (lk && ra1 < N) ? X[xy_at(ra1, l, ldx)] : 0.0;
-      const double b0 = (lk && cb0 < N) ? Yt[xy_at(cb0, l, ldx)] : 0.0;
-      const double b1 = (lk && cb1 < N) ? Yt[xy_at(cb1, l, ldx)] : 0.0;
-      dmma884(acc[0][0][0], acc[0][0][1], a0, b0);
-      dmma884(acc[0][1][0], acc[0][1][1], a0, b1);
-      dmma884(acc[1][0][0], acc[1][0][1], a1, b0);
-      dmma884(acc[1][1][0], acc[1][1][1], a1, b1);
+      double fa[GS], fb[GS];
+#pragma unroll
+      for (int u = 0; u < GS; ++u) {
+        const int ra = r0 + 8 * u + lr, cb = c0 + 8 * u + lr;
+        fa[u] = (lk && ra < N) ? X[xy_at(ra, l, ldx)] : 0.0;
+        fb[u] = (lk && cb < N) ? Yt[xy_at(cb, l, ldx)] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < GS; ++u)
+#pragma unroll
+        for (int v = 0; v < GS; ++v) dmma884(acc[u][v][0], acc[u][v][1], fa[u], fb[v]);
     }
-    double old[2][2][2];
+    double old[GS][GS][2];
 #pragma unroll
-    for (int a = 0; a < 2; ++a)
+    for (int a = 0; a < GS; ++a)
 #pragma unroll
-      for (int b = 0; b < 2; ++b)
+      for (int b = 0; b < GS; ++b)
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
           const int row = r0 + 8 * a + lr, col = c0 + 8 * b + 2 * lc + e;
           old[a][b][e] = (row < N && col < N) ? G[row + (size_t)col * ldg] : 0.0;
         }
 #pragma unroll
-    for (int a = 0; a < 2; ++a)
+    for (int a = 0; a < GS; ++a)
 #pragma unroll
-      for (int b = 0; b < 2; ++b)
+      for (int b = 0; b < GS; ++b)
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
           const int row = r0 + 8 * a + lr, col = c0 + 8 * b + 2 * lc + e;
@@ -648,12 +651,43 @@ __device__ __noinline__ void flush_generic(double *G, int ldg, const double *X, 
   __syncthreads();
 }
 
+// Tile shapes of the rank-2k flush (z2_options.flush_shape_chain).  Every
+// shape forms each element of G with the same k chunks and the same final
+// -acc + old, so they give the same bits; they differ in how the N x N update
+// is cut into warp blocks (load balance over the 8 warps against fragment
+// reuse).  0 picks by divisibility: 24 x 24 blocks when 24 | N, 16 x 16 when
+// 16 | N, else the bounded 16 x 16 groups.
+enum {
+  FS_DEFAULT = 0, FS_GEN16 = 1, FS_GEN8 = 2, FS_T11 = 3, FS_T22 = 4, FS_T33 = 5, FS_T21 = 6,
+  FS_T32 = 7, FS_COUNT = 8
+};
+__host__ __device__ __forceinline__ bool flush_shape_ok(int shape, int N) {
+  switch (shape) {
+    case FS_DEFAULT: case FS_GEN16: case FS_GEN8: return true;
+    case FS_T11: return N % 8 == 0;
+    case FS_T22: case FS_T21: return N % 16 == 0;
+    case FS_T33: return N % 24 == 0;
+    case FS_T32: return N % 48 == 0;
+    default: return false;
+  }
+}
+
 // G <- G - X Yt^T over the m queued columns: one DMMA rank-m update.
 __device__ __forceinline__ void rank_update(double *G, int ldg, const double *X, const double *Yt,
-                                            int N, int ldx, int m) {
+                                            int N, int ldx, int m, int shape = FS_DEFAULT) {
+  switch (shape) {
+    case FS_GEN16: flush_generic<2>(G, ldg, X, Yt, N, ldx, m); return;
+    case FS_GEN8: flush_generic<1>(G, ldg, X, Yt, N, ldx, m); return;
+    case FS_T11: flush_tiles<1, 1>(G, ldg, X, Yt, N, ldx, m); return;
+    case FS_T22: flush_tiles<2, 2>(G, ldg, X, Yt, N, ldx, m); return;
+    case FS_T33: flush_tiles<3, 3>(G, ldg, X, Yt, N, ldx, m); return;
+    case FS_T21: flush_tiles<2, 1>(G, ldg, X, Yt, N, ldx, m); return;
+    case FS_T32: flush_tiles<3, 2>(G, ldg, X, Yt, N, ldx, m); return;
+    default: break;
+  }
   if (N % 24 == 0) flush_tiles<3, 3>(G, ldg, X, Yt, N, ldx, m);
   else if (N % 16 == 0) flush_tiles<2, 2>(G, ldg, X, Yt, N, ldx, m);
-  else flush_generic(G, ldg, X, Yt, N, ldx, m);
+  else flush_generic<2>(G, ldg, X, Yt, N, ldx, m);
 }
 
 // The 2N proposals of one slice (LocalK_prop_L: bonds 2N..1, LocalK_prop_R:
@@ -825,7 +859,7 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
       m += 2;
       if (m >= k2) {
         const long long tf = ph_now();
-        rank_update(G, ldg, X, Yt, N, ldx, m);
+        rank_update(G, ldg, X, Yt, N, ldx, m, c.flush_shape);
         m = 0;
         if (threadIdx.x == 0) c.acc[A_PH0 + PH_FLUSH] += (double)(ph_now() - tf);
       }
@@ -833,7 +867,7 @@ __device__ __noinline__ void propose_slice(const ChainDesc &c, const Smem &s, in
   }
   if (m > 0) {
     const long long tf = ph_now();
-    rank_update(G, ldg, X, Yt, N, ldx, m);
+    rank_update(G, ldg, X, Yt, N, ldx, m, c.flush_shape);
     if (threadIdx.x == 0) c.acc[A_PH0 + PH_FLUSH] += (double)(ph_now() - tf);
   }
   if (threadIdx.x == 0) {

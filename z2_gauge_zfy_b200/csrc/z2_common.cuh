@@ -57,6 +57,7 @@ struct ChainDesc {
   double rb[9];     // boson ratio table [(ds+4)/4 * 3 + (dt+4)/4]
   int use_kin;      // RT > Zero (src/local_sweep.f90:96, dynamics.f90:57)
   int hzero;        // |h| <= Zero (src/local_sweep.f90:64)
+  int flush_shape;  // tile shape of the rank-2k flush (FS_*; 0 = by divisibility)
   int stab_exact;   // 1: the reference's column-pivoted QR in the wraps; 0: the
                     // pre-pivoted blocked QR and scale-split G (z2_stab.cuh)
   int kin_fused;    // L when the bond table has the square-lattice layout of

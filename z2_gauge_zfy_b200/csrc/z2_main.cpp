@@ -352,11 +352,12 @@ int main(int argc, char **argv) {
     cp[c] = z2_chain_params{p.RT, p.J, p.h, p.mu, p.Q, p.Nlx, p.Nly, p.Ltrot, p.beta,
                             p.Nwrap, 1, 1, nullptr};
   z2_options opt{0, 0, device, p.is_tau ? 1 : 0, 1, nullptr};
-  // delayed-update rank from the library's autotuner
-  std::vector<int32_t> kdelay(nch, 0);
-  int r = z2_tune_delay(cp.data(), nch, &opt, kdelay.data());
-  if (r) return fail(nullptr, "z2_tune_delay", r);
+  // delayed-update rank and flush tile shape from the library's autotuner
+  std::vector<int32_t> kdelay(nch, 0), kshape(nch, 0);
+  int r = z2_tune(cp.data(), nch, &opt, kdelay.data(), kshape.data());
+  if (r) return fail(nullptr, "z2_tune", r);
   opt.delay_k_chain = kdelay.data();
+  opt.flush_shape_chain = kshape.data();
   z2_handle *h = nullptr;
   r = z2_create(&h, cp.data(), nch, &opt);
   if (r) return fail(h, "z2_create", r);
