@@ -386,6 +386,8 @@ def main():
     ap.add_argument("--chains", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-single", action="store_true")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="built-in delay ranks and tile shapes (few launches: profiling runs)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -416,7 +418,11 @@ def main():
     # delayed-update rank and flush tile shape per lattice size from the
     # library's autotuner (short probe chains, before the timed region)
     t_tune = time.perf_counter()
-    kchain, schain = tune(chains, local)
+    if args.no_tune:
+        kchain = np.zeros(len(chains), dtype=np.int32)
+        schain = np.zeros(len(chains), dtype=np.int32)
+    else:
+        kchain, schain = tune(chains, local)
     t_tune = time.perf_counter() - t_tune
     b = Z2Batch(chains, device=local, delay_k_chain=kchain, flush_shape_chain=schain)
     b.pre()
@@ -442,8 +448,7 @@ def main():
     for _ in range(args.steps):
         t0 = time.perf_counter()
         ms.append(b.sweep_timed(1, False))
-        for i in range(len(chains)):
-            b.obs_equal(i)
+        b.obs_equal_all()
         wall.append(time.perf_counter() - t0)
         st = [b.stats(i) for i in range(len(chains))]
         a_num += sum(s["accepted"] for s in st)

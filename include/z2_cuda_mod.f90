@@ -48,6 +48,10 @@ module z2_cuda_mod
             import; type(c_ptr), value :: h; integer(c_int32_t), value :: chain
             real(c_double) :: obs(7)
         end function
+        integer(c_int) function z2_get_obs_equal_all(h, obs) bind(C, name="z2_get_obs_equal_all")
+            import; type(c_ptr), value :: h
+            real(c_double) :: obs(7, *)
+        end function
         integer(c_int) function z2_get_obs_tau(h, chain, obs) bind(C, name="z2_get_obs_tau")
             import; type(c_ptr), value :: h; integer(c_int32_t), value :: chain
             real(c_double) :: obs(*)

@@ -126,6 +126,12 @@ int z2_sweep_timed(z2_handle *h, int32_t nsweep, int32_t toggle, float *ms);
 /* ---- readback ---- */
 int z2_get_green(const z2_handle *h, int32_t chain, double *G);
 int z2_get_obs_equal(const z2_handle *h, int32_t chain, double out[Z2_NOBS_EQ]);
+/* The bin observables of every chain, out[nchains][Z2_NOBS_EQ] (chain-major),
+ * gathered on the device and read back with one copy (what z2_get_obs_equal
+ * gives chain by chain; Obs_equal%ave of every rank, src/obser_equal.f90:50-71,
+ * before the driver's MPI reduction).  The first call allocates the gather
+ * buffer. */
+int z2_get_obs_equal_all(z2_handle *h, double *out);
 /* out: Z2_NOBS_TAU arrays of (N, Ltrot) column-major, real parts (the
  * imaginary parts of ObserTau are identically zero for real G). */
 int z2_get_obs_tau(const z2_handle *h, int32_t chain, double *out);

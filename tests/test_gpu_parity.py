@@ -363,3 +363,16 @@ def test_tuner_shapes_valid_and_repeatable():
     for c, k, s in zip(chains, k1, s1):
         assert int(s) in ok[c.N], (c.N, s)
         assert k in (4, 6, 8, 12, 16, 24, 32, 48, 64)
+
+
+def test_obs_equal_all_matches_per_chain_readback():
+    """z2_get_obs_equal_all (one gather, one copy) returns exactly what
+    z2_get_obs_equal returns chain by chain."""
+    chains = [Chain(RT=1.0, J=0.5, h=0.5, Nlx=L, Nly=L, Ltrot=20, beta=2.0, Nwrap=10, seed=s)
+              for L, s in ((4, 1), (6, 2), (8, 3))]
+    with Z2Batch(chains) as b:
+        b.pre()
+        b.sweep(1, False)
+        allv = b.obs_equal_all()
+        per = np.array([list(b.obs_equal(i).values()) for i in range(len(chains))])
+    assert allv.shape == (3, 7) and np.array_equal(allv, per)

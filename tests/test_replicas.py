@@ -1,6 +1,6 @@
 """Replica plumbing on CPU: two gloo ranks each run their own oracle chains
 (distinct seeds), read the bin observables back through the product's
-readback path (Z2Batch.obs_equal over a stand-in library that serves the
+readback path (Z2Batch.obs_equal_all over a stand-in library that serves the
 oracle's values, as bench.py reads its batch) and reduce them and the timing
 exactly as the GPU ranks do with NCCL."""
 import os
@@ -18,15 +18,16 @@ def _free_port():
 
 
 class _ObsLib:
-    """Stand-in library: z2_get_obs_equal writes the given rows into the
-    caller's buffer, as the CUDA library copies a chain's bin observables."""
+    """Stand-in library: z2_get_obs_equal_all writes the given rows into the
+    caller's buffer, as the CUDA library copies every chain's bin observables."""
 
     def __init__(self, rows):
         self.rows = rows
 
-    def z2_get_obs_equal(self, h, chain, buf):
-        for q, v in enumerate(self.rows[chain]):
-            buf[q] = v
+    def z2_get_obs_equal_all(self, h, buf):
+        for c, row in enumerate(self.rows):
+            for q, v in enumerate(row):
+                buf[7 * c + q] = v
         return 0
 
 

@@ -35,7 +35,7 @@ EXPORTS = (
     "z2_propT_R", "z2_propgrT_R", "z2_wrap_pre", "z2_wrap_L", "z2_wrap_R", "z2_wrap_tau",
     "z2_dyn_reset", "z2_prop_slice_L", "z2_prop_slice_R", "z2_sweep_reset",
     "z2_obs_equal_calc", "z2_obs_equal_ave", "z2_obs_tau_calc", "z2_obs_tau_ave",
-    "z2_get_prop", "z2_set_prop", "z2_get_propgr", "z2_tune",
+    "z2_get_prop", "z2_set_prop", "z2_get_propgr", "z2_tune", "z2_get_obs_equal_all",
 )
 # entry points (handle, chain, nt) and (handle, chain) of the state mirrors
 STATE_NT = ("z2_propK_pre", "z2_propK_L", "z2_propK_R", "z2_propgrK_R", "z2_wrap_pre",
@@ -116,6 +116,7 @@ def load():
                                    C.POINTER(i32)]),
         "z2_tune": (C.c_int, [C.POINTER(ChainParams), i32, C.POINTER(Options), C.POINTER(i32),
                              C.POINTER(i32)]),
+        "z2_get_obs_equal_all": (C.c_int, [vp, dp]),
         "z2_wrap_L": (C.c_int, [vp, i32, i32, i32]),
         "z2_wrap_R": (C.c_int, [vp, i32, i32, i32]),
         "z2_sweep_reset": (C.c_int, [vp, i32, i32]),

@@ -270,6 +270,13 @@ class Z2Batch:
         self._c(self.lib.z2_get_obs_equal(self.h, chain, dptr(buf)))
         return dict(zip(OBS_EQ_NAMES, buf.tolist()))
 
+    def obs_equal_all(self) -> np.ndarray:
+        """Bin observables of every chain, [n_chains, 7] in the order of
+        ``OBS_EQ_NAMES`` (``z2_get_obs_equal_all``: one gather, one copy)."""
+        buf = np.empty((len(self.chains), _ffi.Z2_NOBS_EQ))
+        self._c(self.lib.z2_get_obs_equal_all(self.h, dptr(buf)))
+        return buf
+
     def obs_tau(self, chain: int) -> dict:
         N, L, _ = self.dims(chain)
         buf = np.empty(7 * N * L)

@@ -258,6 +258,7 @@ struct z2_handle {
   // per-chain status flags in one array (one readback per launch)
   int *d_status = nullptr;
   std::vector<int> h_status;
+  double *d_obs_all = nullptr;   // [nchains][7] gathered bin observables
   // CUDA graphs of the bin launch, keyed by (nsweep, toggle)
   struct GraphEntry { int nsweep, toggle; cudaGraphExec_t exec; };
   std::vector<GraphEntry> graphs;
@@ -666,6 +667,7 @@ extern "C" int z2_destroy(z2_handle *h) {
   if (h->d_queue) cudaFree(h->d_queue);
   if (h->u_buf) cudaFree(h->u_buf);
   if (h->d_status) cudaFree(h->d_status);
+  if (h->d_obs_all) cudaFree(h->d_obs_all);
   for (auto &g : h->graphs) cudaGraphExecDestroy(g.exec);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
@@ -822,6 +824,31 @@ extern "C" int z2_get_obs_equal(const z2_handle *h, int32_t chain, double out[Z2
   CUDA_TRY(hh, cudaSetDevice(h->device));
   CUDA_TRY(hh, cudaMemcpy(out, h->ch[chain].d.acc + A_BIN0, sizeof(double) * Z2_NOBS_EQ,
                           cudaMemcpyDeviceToHost));
+  return Z2_OK;
+}
+
+// The bin observables of every chain gathered into one buffer, so that a
+// driver reads all of them with one copy after each bin.
+__global__ void z2_gather_obs_kernel(const ChainDesc *descs, int nchains, double *out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nchains * Z2_NOBS_EQ;
+       i += gridDim.x * blockDim.x) {
+    const int c = i / Z2_NOBS_EQ, q = i % Z2_NOBS_EQ;
+    out[i] = descs[c].acc[A_BIN0 + q];
+  }
+}
+
+extern "C" int z2_get_obs_equal_all(z2_handle *h, double *out) {
+  if (!h) return Z2_ERR_ARG;
+  if (!out) return set_err(h, Z2_ERR_ARG, "z2_get_obs_equal_all: null buffer");
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  const size_t n = (size_t)h->nchains * Z2_NOBS_EQ;
+  if (!h->d_obs_all) CUDA_TRY(h, cudaMalloc(&h->d_obs_all, n * sizeof(double)));
+  z2_gather_obs_kernel<<<(int)((n + 255) / 256), 256, 0, h->stream>>>(h->d_desc, h->nchains,
+                                                                       h->d_obs_all);
+  CUDA_TRY(h, cudaGetLastError());
+  CUDA_TRY(h, cudaMemcpyAsync(out, h->d_obs_all, n * sizeof(double), cudaMemcpyDeviceToHost,
+                              h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   return Z2_OK;
 }
 

@@ -21,10 +21,9 @@ def chain_seed(base: int, rank: int, index: int) -> int:
 
 def bin_observables(batch) -> np.ndarray:
     """The bin observables of every chain of a ``Z2Batch`` as an array
-    [n_chains, 7] in the order of ``OBS_EQ_NAMES`` (``z2_get_obs_equal``,
+    [n_chains, 7] in the order of ``OBS_EQ_NAMES`` (``z2_get_obs_equal_all``,
     the fields Obs_equal_ave writes, src/obser_equal.f90:50-71)."""
-    return np.array([list(batch.obs_equal(i).values()) for i in range(len(batch.chains))],
-                    dtype=np.float64)
+    return np.asarray(batch.obs_equal_all(), dtype=np.float64)
 
 
 def reduce_bin_observables(obs: np.ndarray, group=None, device: str = "cpu") -> np.ndarray:
