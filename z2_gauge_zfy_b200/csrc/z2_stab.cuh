@@ -214,30 +214,37 @@ __device__ __noinline__ void dev_stab_green_fast(const Smem &s, int N, int nt, i
       M[i + (size_t)j * ldm] = fma(Rs[i] * W1[i + (size_t)j * N], cs, a);
     }
   }
-  // X = DRb^-1 UR^T
-  for (int j = threadIdx.x / 32; j < N; j += Z2_WARPS)
-    for (int i = threadIdx.x & 31; i < N; i += 32)
-      W2[i + (size_t)j * N] = UR[j + (size_t)i * N] * rRb[i];
   __syncthreads();
-  double *Y = W2;
   if (reg) {
-    // M' = Q' R' in registers; R' kept in W3 (upper), Q' formed (blocked
-    // DORGQR) and applied by one GEMM: Y = Q'^T X
+    // M' = Q' R' in registers; R' kept in W3 (upper) and Q' formed in place
+    // (blocked DORGQR).  Then, all in shared memory, X = Q' R'^-T (the
+    // transpose of M'^-1 = R'^-1 Q'^T) and X(a, b) *= DRb^-1(a) DLb^-1(b), so
+    // that X^T = DLb^-1 M'^-1 DRb^-1; finally G = UL^T (X^T UR^T).
     qr_reg_any(M, ldm, N, tau, s.tile, s.tile_doubles, s.red);
     for (int j = threadIdx.x / 32; j < N; j += Z2_WARPS)
       for (int i = threadIdx.x & 31; i <= j; i += 32) W3[i + (size_t)j * N] = M[i + (size_t)j * ldm];
     __syncthreads();
     blk_orgqr(M, ldm, N, tau, s.tile, s.tile_doubles, s.vec + 4 * N, 4 * N, W1);
-    blk_dmma(N, N, N, 1.0, MatRef{M, ldm, 1}, false, MatRef{W2, 1, N}, false, 0.0, W1, N);
-    blk_trsm_lun_blocked(W3, N, N, W1, N, N);        // Y <- R'^-1 Y
-    Y = W1;
-  } else {
-    geqrf_wp_any(M, ldm, N, tau, W3, s.tile, s.tile_doubles);        // M' = Q' R'
-    ormqr_wp_any(M, ldm, N, W3, W2, N, N, s.tile, s.tile_doubles);   // X <- Q'^T X
-    blk_trsm_lun_blocked(M, ldm, N, W2, N, N);                       // X <- R'^-1 X
+    blk_trsm_rut_inplace(W3, N, N, M, ldm, N);
+    for (int j = threadIdx.x / 32; j < N; j += Z2_WARPS) {
+      const double cl = rLb[j];
+      for (int i = threadIdx.x & 31; i < N; i += 32) M[i + (size_t)j * ldm] *= rRb[i] * cl;
+    }
+    __syncthreads();
+    blk_dmma(N, N, N, 1.0, MatRef{M, ldm, 1}, false, MatRef{UR, N, 1}, false, 0.0, W1, N);
+    blk_dmma(N, N, N, 1.0, MatRef{ULT, 1, N}, false, MatRef{W1, 1, N}, false, 0.0, Gout, N);
+    return;
   }
+  // X = DRb^-1 UR^T
   for (int j = threadIdx.x / 32; j < N; j += Z2_WARPS)
-    for (int i = threadIdx.x & 31; i < N; i += 32) Y[i + (size_t)j * N] *= rLb[i];
+    for (int i = threadIdx.x & 31; i < N; i += 32)
+      W2[i + (size_t)j * N] = UR[j + (size_t)i * N] * rRb[i];
   __syncthreads();
-  blk_dmma(N, N, N, 1.0, MatRef{ULT, 1, N}, false, MatRef{Y, 1, N}, false, 0.0, Gout, N);
+  geqrf_wp_any(M, ldm, N, tau, W3, s.tile, s.tile_doubles);        // M' = Q' R'
+  ormqr_wp_any(M, ldm, N, W3, W2, N, N, s.tile, s.tile_doubles);   // X <- Q'^T X
+  blk_trsm_lun_blocked(M, ldm, N, W2, N, N);                       // X <- R'^-1 X
+  for (int j = threadIdx.x / 32; j < N; j += Z2_WARPS)
+    for (int i = threadIdx.x & 31; i < N; i += 32) W2[i + (size_t)j * N] *= rLb[i];
+  __syncthreads();
+  blk_dmma(N, N, N, 1.0, MatRef{ULT, 1, N}, false, MatRef{W2, 1, N}, false, 0.0, Gout, N);
 }
