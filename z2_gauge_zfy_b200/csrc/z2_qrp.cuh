@@ -395,22 +395,32 @@ __device__ __noinline__ void qrp_reg(double *A, int lda, int n, int *jpvt, doubl
 // trailing columns.  v and tau alternate between two buffers by the parity
 // of j: the warp that writes the buffer of step j + 2 has passed the barrier
 // of step j + 1, which every reader of step j reaches only after its reads.
-// work: >= 2 n doubles; red: >= 32 doubles.
+// work: >= 2 n doubles; red: >= 32 doubles.  perm (optional, 1-based like
+// ZGEQP3's jpvt): factor A P instead of A, column j of A P being column
+// perm[j] - 1 of A.  Every column is read into the register tile before the
+// first finished column is written back, so the permutation costs nothing.
 template <int S>
 __device__ __noinline__ void qr_reg(double *A, int lda, int n, double *tau, double *work,
-                                    double *red) {
+                                    double *red, const int *perm) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int tr = lane & 15, tc = (warp << 1) | (lane >> 4);
   const int hl = lane & 16;
   double *tsh = red + 24;                              // [2] tau of the step
   double a[S][S];
+  int src[S];
+#pragma unroll
+  for (int q = 0; q < S; ++q) {
+    const int c = tc + 16 * q;
+    src[q] = (c < n) ? (perm ? perm[c] - 1 : c) : 0;
+  }
 #pragma unroll
   for (int p = 0; p < S; ++p)
 #pragma unroll
     for (int q = 0; q < S; ++q) {
       const int r = tr + 16 * p, c = tc + 16 * q;
-      a[p][q] = (r < n && c < n) ? A[r + (size_t)c * lda] : 0.0;
+      a[p][q] = (r < n && c < n) ? A[r + (size_t)src[q] * lda] : 0.0;
     }
+  __syncthreads();   // every column read before the first is written back
   unsigned done = 0;   // bit q: column tc + 16 q factored (or outside the matrix)
 #pragma unroll
   for (int q = 0; q < S; ++q)
@@ -529,18 +539,18 @@ __device__ __forceinline__ void blk_geqp3_fast(double *A, int lda, int n, int *j
 // QR without pivoting of the pre-pivoted stabilization, register-resident for
 // n <= 144 (false when the size or the work space does not allow it).
 __device__ __forceinline__ bool qr_reg_any(double *A, int lda, int n, double *tau, double *work,
-                                           int wd, double *red) {
+                                           int wd, double *red, const int *perm = nullptr) {
   if (work == nullptr || wd < 2 * n) return false;
   switch ((n + 15) >> 4) {
-    case 1: qr_reg<1>(A, lda, n, tau, work, red); return true;
-    case 2: qr_reg<2>(A, lda, n, tau, work, red); return true;
-    case 3: qr_reg<3>(A, lda, n, tau, work, red); return true;
-    case 4: qr_reg<4>(A, lda, n, tau, work, red); return true;
-    case 5: qr_reg<5>(A, lda, n, tau, work, red); return true;
-    case 6: qr_reg<6>(A, lda, n, tau, work, red); return true;
-    case 7: qr_reg<7>(A, lda, n, tau, work, red); return true;
-    case 8: qr_reg<8>(A, lda, n, tau, work, red); return true;
-    case 9: qr_reg<9>(A, lda, n, tau, work, red); return true;
+    case 1: qr_reg<1>(A, lda, n, tau, work, red, perm); return true;
+    case 2: qr_reg<2>(A, lda, n, tau, work, red, perm); return true;
+    case 3: qr_reg<3>(A, lda, n, tau, work, red, perm); return true;
+    case 4: qr_reg<4>(A, lda, n, tau, work, red, perm); return true;
+    case 5: qr_reg<5>(A, lda, n, tau, work, red, perm); return true;
+    case 6: qr_reg<6>(A, lda, n, tau, work, red, perm); return true;
+    case 7: qr_reg<7>(A, lda, n, tau, work, red, perm); return true;
+    case 8: qr_reg<8>(A, lda, n, tau, work, red, perm); return true;
+    case 9: qr_reg<9>(A, lda, n, tau, work, red, perm); return true;
     default: return false;
   }
 }

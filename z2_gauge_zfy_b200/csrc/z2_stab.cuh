@@ -162,14 +162,17 @@ __device__ __noinline__ void dev_stab_U_fast(const Smem &s, int N, double *A, in
     jpvt[r] = j + 1;                               // 1-based, as ZGEQP3's jpvt
   }
   __syncthreads();
-  blk_copy(W0, N, A, lda, N, N);                   // A <- A P
-  for (int j = warp; j < N; j += Z2_WARPS) {
-    const double *src = W0 + (size_t)(jpvt[j] - 1) * N;
-    for (int i = lane; i < N; i += 32) A[i + (size_t)j * lda] = src[i];
+  if (reg) {
+    qr_reg_any(A, lda, N, tau, s.tile, s.tile_doubles, s.red, jpvt);   // QR of A P
+  } else {
+    blk_copy(W0, N, A, lda, N, N);                 // A <- A P
+    for (int j = warp; j < N; j += Z2_WARPS) {
+      const double *src = W0 + (size_t)(jpvt[j] - 1) * N;
+      for (int i = lane; i < N; i += 32) A[i + (size_t)j * lda] = src[i];
+    }
+    __syncthreads();
+    geqrf_wp_any(A, lda, N, tau, nullptr, s.tile, s.tile_doubles);
   }
-  __syncthreads();
-  if (reg) qr_reg_any(A, lda, N, tau, s.tile, s.tile_doubles, s.red);
-  else geqrf_wp_any(A, lda, N, tau, nullptr, s.tile, s.tile_doubles);
   blk_qdrp_scale(A, lda, N, Dn, rd);               // D = |R_ii|, R rows /= D
   for (int i = threadIdx.x; i < N; i += Z2_NT) D[i] = Dn[i];
   if (!left) {
