@@ -5,7 +5,7 @@ adjoint, through the C ABI against the oracle (oracle/z2_oracle.py).
   UDV stacks of real chains: UR, DR, VR from Local_sweep_pre's right chain and
   UL, DL, VL from a left half-sweep's stack at the same stabilization point,
   the pair Wrap_tau hands to stab_green_big (src/stabilization.f90:478-514).
-- a toggle bin at N = 144 (sweep_L, sweep_R and Dyn%sweep_R,
+- a toggle bin at N = 144 and N = 256 (sweep_L, sweep_R and Dyn%sweep_R,
   src/dynamics.f90:41-62; propgrK_R, src/multiply.f90:43-63; the seven
   Obs_tau correlators, src/obser_tau.f90:56-133): decisions bit-identical,
   G, the correlators and their momentum-space transforms within 1e-10.
@@ -57,9 +57,12 @@ def test_stab_green_big_at_size(L, Ltrot, Nwrap, st):
     assert max(errs) < RTOL, errs
 
 
-def test_tau_bin_at_N144():
-    ch = Chain(RT=1.0, J=0.5, h=0.5, mu=0.1, Nlx=12, Nly=12, Ltrot=20, beta=2.0, Nwrap=10,
-               seed=1441)
+@pytest.mark.parametrize("L,Ltrot,Nwrap", [(12, 20, 10), (16, 16, 8)])
+def test_tau_bin_at_size(L, Ltrot, Nwrap):
+    """N = 144 (G in shared memory) and N = 256 (G in HBM, the large batched
+    configuration's lattice and Nwrap), a whole toggle bin against the oracle."""
+    ch = Chain(RT=1.0, J=0.5, h=0.5, mu=0.1, Nlx=L, Nly=L, Ltrot=Ltrot, beta=0.1 * Ltrot,
+               Nwrap=Nwrap, seed=1441 + L)
     p = _params(ch)
     c = zo.Z2Chain(p, seed=ch.seed, record_decisions=True)
     c.pre()
@@ -89,7 +92,7 @@ def test_tau_bin_at_N144():
     for q in range(3):
         xo = c.dyn_X[0][q]
         assert abs(st[f"Xmaxm_tau{q}"] - xo) <= 1e-10 + 1e-6 * xo, (q, st[f"Xmaxm_tau{q}"], xo)
-    print(f"tau bin N=144: worst correlator rel error {worst:.2e}")
+    print(f"tau bin N={ch.N}: worst correlator rel error {worst:.2e}")
 
 
 def test_logdet_grad_at_adjoint_size():
