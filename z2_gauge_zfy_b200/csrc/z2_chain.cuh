@@ -1024,6 +1024,28 @@ __device__ __noinline__ void load_G(const ChainDesc &c, const Smem &s) {
   if (c.g_in_smem) blk_copy(s.G, s.ldg, c.G, c.N, c.N, c.N);
 }
 
+// The stabilized Green's function Gn replaces the propagated one in one pass
+// over both: returns the drift max |Gn - G| (compare_mat,
+// src/stabilization.f90:365-372) and leaves G = Gn in global memory and, for
+// a chain whose G lives in shared memory, there too.
+__device__ __noinline__ double take_green(const ChainDesc &c, const Smem &s, const double *Gn) {
+  const int N = c.N, ldg = s.ldg;
+  double *Gg = c.G, *Gs = s.G;
+  const bool sm = c.g_in_smem != 0;
+  double m = 0.0;
+  blk_walk<8, double2>(
+      N, N, [&](int i, int j) { return make_double2(Gn[i + (size_t)j * N], Gg[i + (size_t)j * N]); },
+      [&](double2 v, int i, int j) {
+        const double d = fabs(v.x - v.y);
+        m = (d > m || d != d) ? d : m;   // keep NaN visible
+        Gg[i + (size_t)j * N] = v.x;
+        if (sm) Gs[i + (size_t)j * ldg] = v.x;
+      });
+  const double r = blk_max(m, s.red);
+  __syncthreads();
+  return r;
+}
+
 __device__ __noinline__ void copy_vec(double *dst, const double *src, int n) {
   for (int i = threadIdx.x; i < n; i += Z2_NT) dst[i] = src[i];
   __syncthreads();
@@ -1095,15 +1117,13 @@ __device__ __noinline__ void wrap_L(const ChainDesc &c, const Smem &s, int nt, P
   if (nt != c.Ltrot) {
     { PhTimer t(c, PH_STABU); chain_stab_U(c, s, A, lda, c.ULT, c.DL, c.VL, true); }
     { PhTimer t(c, PH_STABG); chain_stab_green(c, s, nt, A, lda, c.W3); }
-    double dif = blk_maxdiff(c.W3, N, c.G, N, N, s.red);
-    record_drift(c, dif, stats);
-    blk_copy(c.G, N, c.W3, N, N, N);
+    record_drift(c, take_green(c, s, c.W3), stats);
   }
   { PhTimer t(c, PH_STACK);
     blk_copy(c.ULTs + (size_t)st * NN, N, c.ULT, N, N, N);
     blk_copy(c.VLs + (size_t)st * NN, N, c.VL, N, N, N);
     copy_vec(c.DLs + (size_t)st * N, c.DL, N); }
-  load_G(c, s);
+  if (nt == c.Ltrot) load_G(c, s);   // otherwise take_green reloaded it
 }
 
 // Wrap_R (src/stabilization.f90:439-476)
@@ -1127,14 +1147,12 @@ __device__ __noinline__ void wrap_R(const ChainDesc &c, const Smem &s, int nt, P
   if (nt != 0) {
     { PhTimer t(c, PH_STABU); chain_stab_U(c, s, A, lda, c.UR, c.DR, c.VR, false); }
     { PhTimer t(c, PH_STABG); chain_stab_green(c, s, nt, A, lda, c.W3); }
-    double dif = blk_maxdiff(c.W3, N, c.G, N, N, s.red);
-    record_drift(c, dif, stats);
-    blk_copy(c.G, N, c.W3, N, N, N);
+    record_drift(c, take_green(c, s, c.W3), stats);
   }
   { PhTimer t(c, PH_STACK);
     blk_copy(c.URs + (size_t)st * NN, N, c.UR, N, N, N);
     blk_copy(c.VRs + (size_t)st * NN, N, c.VR, N, N, N);
     copy_vec(c.DRs + (size_t)st * N, c.DR, N); }
-  load_G(c, s);
+  if (nt == 0) load_G(c, s);   // otherwise take_green reloaded it
 }
 

@@ -19,6 +19,35 @@ __device__ __forceinline__ double dlapy2(double x, double y) {
   return w * sqrt(1.0 + q * q);
 }
 
+// Element walk over an m x n column-major block whose operands sit in L2 or
+// HBM: the elements are dealt to the threads in column-major order
+// (consecutive threads take consecutive rows, so accesses stay coalesced), B
+// per thread at a time, and every batch issues its B loads before any use.  ld(i, j) returns
+// the element's operands, use(v, i, j) consumes them.
+template <int B, class T, class Ld, class Use>
+__device__ __forceinline__ void blk_walk(int m, int n, Ld ld, Use use) {
+  if (m <= 0 || n <= 0) return;
+  const int dj = Z2_NT / m, di = Z2_NT % m;
+  int i = threadIdx.x % m, j = threadIdx.x / m;
+  const long long total = (long long)m * n;
+  for (long long e0 = 0; e0 < total; e0 += (long long)B * Z2_NT) {
+    int ii[B], jj[B];
+    T v[B];
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+      ii[b] = i;
+      jj[b] = j;
+      if (j < n) v[b] = ld(i, j);
+      i += di;
+      j += dj;
+      if (i >= m) { i -= m; ++j; }
+    }
+#pragma unroll
+    for (int b = 0; b < B; ++b)
+      if (jj[b] < n) use(v[b], ii[b], jj[b]);
+  }
+}
+
 // Element copies are issued in batches of 4 loads before 4 stores (dst and
 // src may be the same allocation, so the compiler keeps program order).
 __device__ __noinline__ void blk_copy(double *dst, int ldd, const double *src, int lds, int m, int n) {

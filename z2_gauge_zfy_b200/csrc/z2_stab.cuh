@@ -210,13 +210,12 @@ __device__ __noinline__ void dev_stab_green_fast(const Smem &s, int N, int nt, i
   blk_dmma(N, N, N, 1.0, MatRef{UR, N, 1}, false, MatRef{ULT, 1, N}, false, 0.0, M, ldm);
   blk_dmma(N, N, N, 1.0, MatRef{VR, 1, N}, false, MatRef{VL, 1, N}, false, 0.0, W1, N);
   // M' = DRb^-1 (UR^T UL^T) DLb^-1 + DRs (VR VL) DLs
-  for (int j = threadIdx.x / 32; j < N; j += Z2_WARPS) {
-    const double cb = rLb[j], cs = Ls[j];
-    for (int i = threadIdx.x & 31; i < N; i += 32) {
-      const double a = M[i + (size_t)j * ldm] * rRb[i] * cb;
-      M[i + (size_t)j * ldm] = fma(Rs[i] * W1[i + (size_t)j * N], cs, a);
-    }
-  }
+  blk_walk<8, double2>(
+      N, N, [&](int i, int j) { return make_double2(M[i + (size_t)j * ldm], W1[i + (size_t)j * N]); },
+      [&](double2 v, int i, int j) {
+        const double a = v.x * rRb[i] * rLb[j];
+        M[i + (size_t)j * ldm] = fma(Rs[i] * v.y, Ls[j], a);
+      });
   __syncthreads();
   if (reg) {
     // M' = Q' R' in registers; R' kept in W3 (upper) and Q' formed in place
