@@ -1,6 +1,7 @@
 // z2_stab.cuh -- UDV stabilization (src/stabilization.f90:42-200) on the
 // DMMA GEMM, the register-resident pivoted QR and the blocked DORGQR.
 #pragma once
+#include "z2_lu.cuh"
 #include "z2_qrf.cuh"
 #include "z2_qrp.cuh"
 
@@ -109,10 +110,12 @@ __device__ __noinline__ void dev_stab_green(const Smem &s, int N, int nt, int Lt
 //   M  = UR^T UL^T + DR (VR VL) DL
 //      = DRb (DRb^-1 UR^T UL^T DLb^-1 + DRs VR VL DLs) DLb = DRb M' DLb,
 //   DRb = max(DR, 1), DRs = min(DR, 1) (DLb, DLs likewise),
-//   G  = UL^T M^-1 UR^T = UL^T DLb^-1 R'^-1 Q'^T DRb^-1 UR^T,   M' = Q' R',
-// where M' has entries of order one, so its QR needs no pivoting.  U, D, V and
-// G are the same as the reference's up to rounding (the UDV factors of a
-// product are not unique: the column order of D may differ).
+//   G  = UL^T M^-1 UR^T = UL^T DLb^-1 M'^-1 DRb^-1 UR^T,
+// where M' has entries of order one.  M' is only inverted: for N <= 144 in
+// registers by Gauss-Jordan elimination with partial pivoting, above that
+// through the blocked Householder QR without pivoting (M' = Q' R').  U, D, V and G are the same as the reference's up to
+// rounding (the UDV factors of a product are not unique: the column order of
+// D may differ).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ bool qrf_ok(int n, int wd) { return n <= 256 && qrf_ncb(n, wd) > 0; }
 
@@ -194,7 +197,7 @@ __device__ __noinline__ void dev_stab_green_fast(const Smem &s, int N, int nt, i
                                                  const double *DL, const double *VL, double *M,
                                                  int ldm, double *W1, double *W2, double *W3,
                                                  double *Gout) {
-  const bool reg = N <= 144 && s.tile_doubles >= 2 * N;   // register-resident QR
+  const bool reg = N <= 144 && s.tile_doubles >= 4 * N;   // register-resident inverse
   if (!reg && !qrf_ok(N, s.tile_doubles)) {
     dev_stab_green(s, N, nt, Ltrot, UR, DR, VR, ULT, DL, VL, M, ldm, W1, W2, W3, Gout);
     return;
@@ -218,22 +221,18 @@ __device__ __noinline__ void dev_stab_green_fast(const Smem &s, int N, int nt, i
       });
   __syncthreads();
   if (reg) {
-    // M' = Q' R' in registers; R' kept in W3 (upper) and Q' formed in place
-    // (blocked DORGQR).  Then, all in shared memory, X = Q' R'^-T (the
-    // transpose of M'^-1 = R'^-1 Q'^T) and X(a, b) *= DRb^-1(a) DLb^-1(b), so
-    // that X^T = DLb^-1 M'^-1 DRb^-1; finally G = UL^T (X^T UR^T).
-    qr_reg_any(M, ldm, N, tau, s.tile, s.tile_doubles, s.red);
-    for (int j = threadIdx.x / 32; j < N; j += Z2_WARPS)
-      for (int i = threadIdx.x & 31; i <= j; i += 32) W3[i + (size_t)j * N] = M[i + (size_t)j * ldm];
+    // M' is inverted in place in registers (Gauss-Jordan with partial
+    // pivoting): on exit row j of M is DLb^-1(j) T(piv j, :) with
+    // DLb^-1 M'^-1 = M P, P(m, k) = 1 iff piv[m] = k.  Then
+    //   Y = P DRb^-1 UR^T,  Y(m, c) = DRb^-1(piv m) UR(c, piv m)  (stored
+    //   transposed in W2, both sides coalesced),  W1 = M Y,  G = UL^T W1.
+    int *piv = s.ivec;
+    gj_reg_any(M, ldm, N, piv, rLb, s.tile, s.tile_doubles, s.red);
+    blk_walk<8, double>(
+        N, N, [&](int c, int m) { return UR[c + (size_t)piv[m] * N]; },
+        [&](double v, int c, int m) { W2[c + (size_t)m * N] = v * rRb[piv[m]]; });
     __syncthreads();
-    blk_orgqr(M, ldm, N, tau, s.tile, s.tile_doubles, s.vec + 4 * N, 4 * N, W1);
-    blk_trsm_rut_inplace(W3, N, N, M, ldm, N);
-    for (int j = threadIdx.x / 32; j < N; j += Z2_WARPS) {
-      const double cl = rLb[j];
-      for (int i = threadIdx.x & 31; i < N; i += 32) M[i + (size_t)j * ldm] *= rRb[i] * cl;
-    }
-    __syncthreads();
-    blk_dmma(N, N, N, 1.0, MatRef{M, ldm, 1}, false, MatRef{UR, N, 1}, false, 0.0, W1, N);
+    blk_dmma(N, N, N, 1.0, MatRef{M, 1, ldm}, false, MatRef{W2, N, 1}, false, 0.0, W1, N);
     blk_dmma(N, N, N, 1.0, MatRef{ULT, 1, N}, false, MatRef{W1, 1, N}, false, 0.0, Gout, N);
     return;
   }
