@@ -28,10 +28,12 @@ struct MatRef {
 
 // C (m x n, column-major ldc) = alpha * A (m x k) B (k x n) + beta * C.
 // a_upper: A(i, l) reads as 0 for i > l; b_lower: B(l, j) reads as 0 for l < j
-// (B = R^T of an upper-triangular R).  Operands may live in shared or global
-// memory.  Each warp owns 16 x 16 groups of 8 x 8 DMMA tiles; interior groups
-// run a pointer-increment loop without bounds checks.  beta == 0 never reads
-// C.  Ends with the block synchronised.
+// (B = R^T of an upper-triangular R); a group's k loop then starts at its
+// first row (a_upper) or column (b_lower), below which every term is zero.
+// Operands may live in shared or global memory.  Each warp owns 16 x 16
+// groups of 8 x 8 DMMA tiles; interior groups run a pointer-increment loop
+// without bounds checks.  beta == 0 never reads C.  Ends with the block
+// synchronised.
 __device__ __noinline__ void blk_dmma(int m, int n, int k, double alpha, MatRef A, bool a_upper,
                                      MatRef B, bool b_lower, double beta, double *C, int ldc) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -47,11 +49,13 @@ __device__ __noinline__ void blk_dmma(int m, int n, int k, double alpha, MatRef 
       for (int b = 0; b < 2; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
     const int ra0 = r0 + lr, ra1 = r0 + 8 + lr;
     const int cb0 = c0 + lr, cb1 = c0 + 8 + lr;
+    int lbeg = a_upper ? r0 : 0;   // a multiple of 16
+    if (b_lower && c0 > lbeg) lbeg = c0;
     const bool full = (k & 3) == 0 && (r0 + 16 <= m) && (c0 + 16 <= n);
     if (full) {
-      const double *pa0 = A.p + (size_t)ra0 * A.rs + (size_t)lc * A.cs;
+      const double *pa0 = A.p + (size_t)ra0 * A.rs + (size_t)(lbeg + lc) * A.cs;
       const double *pa1 = pa0 + (size_t)8 * A.rs;
-      const double *pb0 = B.p + (size_t)lc * B.rs + (size_t)cb0 * B.cs;
+      const double *pb0 = B.p + (size_t)(lbeg + lc) * B.rs + (size_t)cb0 * B.cs;
       const double *pb1 = pb0 + (size_t)8 * B.cs;
       const size_t sa = (size_t)4 * A.cs, sb = (size_t)4 * B.rs;
       if (plain) {
@@ -68,7 +72,7 @@ __device__ __noinline__ void blk_dmma(int m, int n, int k, double alpha, MatRef 
         // triangular operand: the same loop with the masked entries zeroed
         // (no bounds checks inside a full tile)
 #pragma unroll 4
-        for (int l0 = 0; l0 < k; l0 += 4) {
+        for (int l0 = lbeg; l0 < k; l0 += 4) {
           const int l = l0 + lc;
           double a0 = *pa0, a1 = *pa1, b0 = *pb0, b1 = *pb1;
           pa0 += sa; pa1 += sa; pb0 += sb; pb1 += sb;
@@ -82,7 +86,7 @@ __device__ __noinline__ void blk_dmma(int m, int n, int k, double alpha, MatRef 
       }
     } else {
 #pragma unroll 4
-      for (int l0 = 0; l0 < k; l0 += 4) {
+      for (int l0 = lbeg; l0 < k; l0 += 4) {
         const int l = l0 + lc;
         const bool lk = l < k;
         double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;

@@ -116,12 +116,45 @@ __device__ __noinline__ void scale_G_mu(const ChainDesc &c, const Smem &s) {
   }
 }
 
+// Asks L2 for n doubles at p, one 128-byte line per prefetch, the lines
+// spread over the block (a hint: nothing waits for it).
+__device__ __forceinline__ void l2_prefetch(const double *p, int n) {
+  const char *b = reinterpret_cast<const char *>(p);
+  const size_t bytes = (size_t)n * sizeof(double);
+  for (size_t o = (size_t)threadIdx.x * 128; o < bytes; o += (size_t)Z2_NT * 128)
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(b + o));
+}
+
+// The matrices a wrap reads from global memory, fetched into L2 about a
+// slice ahead of it: the stack entry st of the other sweep direction (kept
+// since the previous sweep) and this direction's U, V, D (from the previous
+// wrap), which other chains' traffic has usually evicted by then.
+__device__ __noinline__ void prefetch_wrap(const ChainDesc &c, int st, bool left) {
+  const int N = c.N, NN = N * N;
+  if (left) {
+    l2_prefetch(c.URs + (size_t)st * NN, NN);
+    l2_prefetch(c.VRs + (size_t)st * NN, NN);
+    l2_prefetch(c.DRs + (size_t)st * N, N);
+    l2_prefetch(c.ULT, NN);
+    l2_prefetch(c.VL, NN);
+    l2_prefetch(c.DL, N);
+  } else {
+    l2_prefetch(c.ULTs + (size_t)st * NN, NN);
+    l2_prefetch(c.VLs + (size_t)st * NN, NN);
+    l2_prefetch(c.DLs + (size_t)st * N, N);
+    l2_prefetch(c.UR, NN);
+    l2_prefetch(c.VR, NN);
+    l2_prefetch(c.DR, N);
+  }
+}
+
 // Local_sweep_L (src/local_sweep.f90:106-124)
 __device__ __noinline__ void sweep_L(const ChainDesc &c, const Smem &s) {
   const int N = c.N;
   Pend pd{1, 0};
   for (int nt = c.Ltrot; nt >= 1; --nt) {
     if (nt % c.Nwrap == 0) { PhTimer t(c, PH_WRAP); wrap_L(c, s, nt, pd, true); }
+    if ((nt - 1) % c.Nwrap == 0) prefetch_wrap(c, (nt - 1) / c.Nwrap, true);
     { PhTimer t(c, PH_OBS); obs_equal(c, s, nt); }
     scale_G_mu(c, s);                               // propT_L
     { PhTimer t(c, PH_PROP); propose_slice(c, s, nt, true, 0); }   // bonds 2N..1
@@ -148,6 +181,7 @@ __device__ __noinline__ void sweep_R(const ChainDesc &c, const Smem &s, bool tog
   Pend pd{1, 0};
   { PhTimer t(c, PH_WRAP); wrap_R(c, s, 0, pd, true); }
   for (int nt = 1; nt <= c.Ltrot; ++nt) {
+    if (nt % c.Nwrap == 0) prefetch_wrap(c, nt / c.Nwrap, false);
     {
       PhTimer t(c, PH_KIN);
       build_table(c, s, nt);
