@@ -62,7 +62,7 @@ class ChainSpec:
 
 # DRAM bytes (read + write) of one step of the 256-chain workload, from one
 # ncu capture of the chain kernel (dram__bytes_read.sum + dram__bytes_write.sum)
-TRAFFIC_BYTES_PER_STEP = 2844271872 + 4710838528
+TRAFFIC_BYTES_PER_STEP = 3254171904 + 5548485632
 
 
 def batched_chains(rank: int = 0, n: int = 256):

@@ -30,7 +30,10 @@ struct MatRef {
 // a_upper: A(i, l) reads as 0 for i > l; b_lower: B(l, j) reads as 0 for l < j
 // (B = R^T of an upper-triangular R); a group's k loop then starts at its
 // first row (a_upper) or column (b_lower), below which every term is zero.
-// Operands may live in shared or global memory.  Each warp owns 16 x 16
+// When an operand's k index is contiguous (B column-major, or A seen
+// transposed), interior groups of a plain product take it as 16-byte loads
+// covering two k steps (the k order within each group of 8 changes, not the
+// terms).  Operands may live in shared or global memory.  Each warp owns 16 x 16
 // groups of 8 x 8 DMMA tiles; interior groups run a pointer-increment loop
 // without bounds checks.  beta == 0 never reads C.  Ends with the block
 // synchronised.
@@ -40,6 +43,11 @@ __device__ __noinline__ void blk_dmma(int m, int n, int k, double alpha, MatRef 
   const int lr = lane >> 2, lc = lane & 3;
   const int gm = (m + 15) >> 4, gn = (n + 15) >> 4;
   const bool plain = !a_upper && !b_lower && (k & 3) == 0;
+  // 16-byte operand loads: k contiguous, the matrix 16-byte aligned and its
+  // other stride even (so every lane's pair starts on a 16-byte boundary)
+  const bool va = A.cs == 1 && (A.rs & 1) == 0 && ((uintptr_t)A.p & 15) == 0;
+  const bool vb = B.rs == 1 && (B.cs & 1) == 0 && ((uintptr_t)B.p & 15) == 0;
+  const bool pair = (k & 7) == 0 && (va || vb);
   for (int g = warp; g < gm * gn; g += Z2_WARPS) {
     const int r0 = (g % gm) << 4, c0 = (g / gm) << 4;
     double acc[2][2][2];
@@ -58,7 +66,43 @@ __device__ __noinline__ void blk_dmma(int m, int n, int k, double alpha, MatRef 
       const double *pb0 = B.p + (size_t)(lbeg + lc) * B.rs + (size_t)cb0 * B.cs;
       const double *pb1 = pb0 + (size_t)8 * B.cs;
       const size_t sa = (size_t)4 * A.cs, sb = (size_t)4 * B.rs;
-      if (plain) {
+      if (plain && pair) {
+        // two k steps per pass over 8 k values: lane lc takes k = l0 + 2 lc in
+        // the first and l0 + 2 lc + 1 in the second, so an operand whose k is
+        // contiguous arrives as one 16-byte load for both
+        const double *qa0 = A.p + (size_t)ra0 * A.rs + (size_t)(2 * lc) * A.cs;
+        const double *qa1 = qa0 + (size_t)8 * A.rs;
+        const double *qb0 = B.p + (size_t)(2 * lc) * B.rs + (size_t)cb0 * B.cs;
+        const double *qb1 = qb0 + (size_t)8 * B.cs;
+        const size_t ta = (size_t)8 * A.cs, tb = (size_t)8 * B.rs;
+#pragma unroll 2
+        for (int l0 = 0; l0 < k; l0 += 8) {
+          double2 x0, x1, y0, y1;
+          if (va) {
+            x0 = *reinterpret_cast<const double2 *>(qa0);
+            x1 = *reinterpret_cast<const double2 *>(qa1);
+          } else {
+            x0 = make_double2(qa0[0], qa0[A.cs]);
+            x1 = make_double2(qa1[0], qa1[A.cs]);
+          }
+          if (vb) {
+            y0 = *reinterpret_cast<const double2 *>(qb0);
+            y1 = *reinterpret_cast<const double2 *>(qb1);
+          } else {
+            y0 = make_double2(qb0[0], qb0[B.rs]);
+            y1 = make_double2(qb1[0], qb1[B.rs]);
+          }
+          qa0 += ta; qa1 += ta; qb0 += tb; qb1 += tb;
+          dmma884(acc[0][0][0], acc[0][0][1], x0.x, y0.x);
+          dmma884(acc[0][1][0], acc[0][1][1], x0.x, y1.x);
+          dmma884(acc[1][0][0], acc[1][0][1], x1.x, y0.x);
+          dmma884(acc[1][1][0], acc[1][1][1], x1.x, y1.x);
+          dmma884(acc[0][0][0], acc[0][0][1], x0.y, y0.y);
+          dmma884(acc[0][1][0], acc[0][1][1], x0.y, y1.y);
+          dmma884(acc[1][0][0], acc[1][0][1], x1.y, y0.y);
+          dmma884(acc[1][1][0], acc[1][1][1], x1.y, y1.y);
+        }
+      } else if (plain) {
 #pragma unroll 4
         for (int l0 = 0; l0 < k; l0 += 4) {
           const double a0 = *pa0, a1 = *pa1, b0 = *pb0, b1 = *pb1;

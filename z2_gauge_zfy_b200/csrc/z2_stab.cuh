@@ -224,15 +224,16 @@ __device__ __noinline__ void dev_stab_green_fast(const Smem &s, int N, int nt, i
     // M' is inverted in place in registers (Gauss-Jordan with partial
     // pivoting): on exit row j of M is DLb^-1(j) T(piv j, :) with
     // DLb^-1 M'^-1 = M P, P(m, k) = 1 iff piv[m] = k.  Then
-    //   Y = P DRb^-1 UR^T,  Y(m, c) = DRb^-1(piv m) UR(c, piv m)  (stored
-    //   transposed in W2, both sides coalesced),  W1 = M Y,  G = UL^T W1.
+    //   Y = P DRb^-1 UR^T,  Y(m, c) = DRb^-1(piv m) UR(c, piv m)  (in W2,
+    //   column-major, so that the GEMM reads its k index contiguously),
+    //   W1 = M Y,  G = UL^T W1.
     int *piv = s.ivec;
     gj_reg_any(M, ldm, N, piv, rLb, s.tile, s.tile_doubles, s.red);
     blk_walk<8, double>(
         N, N, [&](int c, int m) { return UR[c + (size_t)piv[m] * N]; },
-        [&](double v, int c, int m) { W2[c + (size_t)m * N] = v * rRb[piv[m]]; });
+        [&](double v, int c, int m) { W2[m + (size_t)c * N] = v * rRb[piv[m]]; });
     __syncthreads();
-    blk_dmma(N, N, N, 1.0, MatRef{M, 1, ldm}, false, MatRef{W2, N, 1}, false, 0.0, W1, N);
+    blk_dmma(N, N, N, 1.0, MatRef{M, 1, ldm}, false, MatRef{W2, 1, N}, false, 0.0, W1, N);
     blk_dmma(N, N, N, 1.0, MatRef{ULT, 1, N}, false, MatRef{W1, 1, N}, false, 0.0, Gout, N);
     return;
   }
