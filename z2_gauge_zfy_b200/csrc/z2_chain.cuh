@@ -534,11 +534,10 @@ __device__ __forceinline__ size_t xy_at(int i, int q, int ldx) {
 }
 
 // G <- G - X Yt^T over the m queued columns (paired layout) when 8 TR and 8 TC
-// divide N: each warp owns (8 TR) x (8 TC) blocks of G, reads their old
-// values before its DMMA chain (the load latency overlaps the products) and
-// reuses each X fragment TC times and each Yt fragment TR times.  The k loop
-// and the final -acc + old are those of blk_dmma, so the result is the same
-// to the bit.
+// divide N: each warp owns (8 TR) x (8 TC) blocks of G, loads their old
+// values straight into the DMMA accumulators and adds (-X) Yt^T to them in
+// chunks of 4 columns, reusing each X fragment TC times and each Yt fragment
+// TR times.
 template <int TR, int TC>
 __device__ __noinline__ void flush_tiles(double *G, int ldg, const double *X, const double *Yt,
                                          int N, int ldx, int m) {
@@ -550,23 +549,20 @@ __device__ __noinline__ void flush_tiles(double *G, int ldg, const double *X, co
   for (int g = warp; g < gr * gcn; g += Z2_WARPS) {
     const int r0 = (g % gr) * 8 * TR, c0 = (g / gr) * 8 * TC;
     double *cp = G + r0 + lr + (size_t)(c0 + 2 * lc) * ldg;
-    double old[TR][TC][2], acc[TR][TC][2];
+    double acc[TR][TC][2];
 #pragma unroll
     for (int a = 0; a < TR; ++a)
 #pragma unroll
       for (int b = 0; b < TC; ++b)
 #pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          old[a][b][e] = cp[8 * a + (size_t)(8 * b + e) * ldg];
-          acc[a][b][e] = 0.0;
-        }
+        for (int e = 0; e < 2; ++e) acc[a][b][e] = cp[8 * a + (size_t)(8 * b + e) * ldg];
     const double *pa = X + xy_at(r0 + lr, lc, ldx);
     const double *pb = Yt + xy_at(c0 + lr, lc, ldx);
 #pragma unroll 2
     for (int l0 = 0; l0 < m4; l0 += 4) {
       double fa[TR], fb[TC];
 #pragma unroll
-      for (int u = 0; u < TR; ++u) fa[u] = pa[16 * u];
+      for (int u = 0; u < TR; ++u) fa[u] = -pa[16 * u];
 #pragma unroll
       for (int v = 0; v < TC; ++v) fb[v] = pb[16 * v];
       pa += s4; pb += s4;
@@ -580,7 +576,7 @@ __device__ __noinline__ void flush_tiles(double *G, int ldg, const double *X, co
       const bool ok = lc < m - m4;
       double fa[TR], fb[TC];
 #pragma unroll
-      for (int u = 0; u < TR; ++u) fa[u] = ok ? pa[16 * u] : 0.0;
+      for (int u = 0; u < TR; ++u) fa[u] = ok ? -pa[16 * u] : 0.0;
 #pragma unroll
       for (int v = 0; v < TC; ++v) fb[v] = ok ? pb[16 * v] : 0.0;
 #pragma unroll
@@ -593,13 +589,12 @@ __device__ __noinline__ void flush_tiles(double *G, int ldg, const double *X, co
 #pragma unroll
       for (int b = 0; b < TC; ++b)
 #pragma unroll
-        for (int e = 0; e < 2; ++e) cp[8 * a + (size_t)(8 * b + e) * ldg] = -acc[a][b][e] + old[a][b][e];
+        for (int e = 0; e < 2; ++e) cp[8 * a + (size_t)(8 * b + e) * ldg] = acc[a][b][e];
   }
   __syncthreads();
 }
 
-// The same update for any N: (8 GS) x (8 GS) groups with bounds checks (the k
-// loop and epilogue of blk_dmma's general path).
+// The same update for any N: (8 GS) x (8 GS) groups with bounds checks.
 template <int GS>
 __device__ __noinline__ void flush_generic(double *G, int ldg, const double *X, const double *Yt,
                                            int N, int ldx, int m) {
@@ -612,7 +607,12 @@ __device__ __noinline__ void flush_generic(double *G, int ldg, const double *X, 
 #pragma unroll
     for (int a = 0; a < GS; ++a)
 #pragma unroll
-      for (int b = 0; b < GS; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+      for (int b = 0; b < GS; ++b)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int row = r0 + 8 * a + lr, col = c0 + 8 * b + 2 * lc + e;
+          acc[a][b][e] = (row < N && col < N) ? G[row + (size_t)col * ldg] : 0.0;
+        }
     for (int l0 = 0; l0 < m; l0 += 4) {
       const int l = l0 + lc;
       const bool lk = l < m;
@@ -620,7 +620,7 @@ __device__ __noinline__ void flush_generic(double *G, int ldg, const double *X, 
 #pragma unroll
       for (int u = 0; u < GS; ++u) {
         const int ra = r0 + 8 * u + lr, cb = c0 + 8 * u + lr;
-        fa[u] = (lk && ra < N) ? X[xy_at(ra, l, ldx)] : 0.0;
+        fa[u] = (lk && ra < N) ? -X[xy_at(ra, l, ldx)] : 0.0;
         fb[u] = (lk && cb < N) ? Yt[xy_at(cb, l, ldx)] : 0.0;
       }
 #pragma unroll
@@ -628,7 +628,6 @@ __device__ __noinline__ void flush_generic(double *G, int ldg, const double *X, 
 #pragma unroll
         for (int v = 0; v < GS; ++v) dmma884(acc[u][v][0], acc[u][v][1], fa[u], fb[v]);
     }
-    double old[GS][GS][2];
 #pragma unroll
     for (int a = 0; a < GS; ++a)
 #pragma unroll
@@ -636,24 +635,15 @@ __device__ __noinline__ void flush_generic(double *G, int ldg, const double *X, 
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
           const int row = r0 + 8 * a + lr, col = c0 + 8 * b + 2 * lc + e;
-          old[a][b][e] = (row < N && col < N) ? G[row + (size_t)col * ldg] : 0.0;
-        }
-#pragma unroll
-    for (int a = 0; a < GS; ++a)
-#pragma unroll
-      for (int b = 0; b < GS; ++b)
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          const int row = r0 + 8 * a + lr, col = c0 + 8 * b + 2 * lc + e;
-          if (row < N && col < N) G[row + (size_t)col * ldg] = -acc[a][b][e] + old[a][b][e];
+          if (row < N && col < N) G[row + (size_t)col * ldg] = acc[a][b][e];
         }
   }
   __syncthreads();
 }
 
 // Tile shapes of the rank-2k flush (z2_options.flush_shape_chain).  Every
-// shape forms each element of G with the same k chunks and the same final
-// -acc + old, so they give the same bits; they differ in how the N x N update
+// shape forms each element of G from its old value with the same k chunks,
+// so they give the same bits; they differ in how the N x N update
 // is cut into warp blocks (load balance over the 8 warps against fragment
 // reuse).  0 picks by divisibility: 24 x 24 blocks when 24 | N, 16 x 16 when
 // 16 | N, else the bounded 16 x 16 groups.
