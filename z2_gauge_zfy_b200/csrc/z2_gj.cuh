@@ -1,4 +1,4 @@
-// z2_lu.cuh -- register-resident matrix inverse by Gauss-Jordan elimination
+// z2_gj.cuh -- register-resident matrix inverse by Gauss-Jordan elimination
 // with partial pivoting, for the middle matrix of the pre-pivoted
 // stabilization.
 //
@@ -13,19 +13,19 @@
 #pragma once
 #include "z2_qrp.cuh"
 
-#define LU_COL(Q) \
+#define GJ_COL(Q) \
   case Q:         \
     if (Q < S) {  \
       _Pragma("unroll") for (int p = 0; p < S; ++p) col[p] = a[p][Q < S ? Q : 0]; \
     }             \
     break;
-#define LU_ROW(P) \
+#define GJ_ROW(P) \
   case P:         \
     if (P < S) {  \
       _Pragma("unroll") for (int q = 0; q < S; ++q) rowv[q] = a[P < S ? P : 0][q]; \
     }             \
     break;
-#define LU_PICK(P) \
+#define GJ_PICK(P) \
   case P:          \
     if (P < S) cv = col[P < S ? P : 0]; \
     break;
@@ -88,7 +88,7 @@ __device__ __noinline__ void gj_reg(double *A, int lda, int n, int *piv, const d
 #pragma unroll
       for (int p = 0; p < S; ++p) col[p] = 0.0;
       switch (qj) {
-        LU_COL(0) LU_COL(1) LU_COL(2) LU_COL(3) LU_COL(4) LU_COL(5) LU_COL(6) LU_COL(7) LU_COL(8)
+        GJ_COL(0) GJ_COL(1) GJ_COL(2) GJ_COL(3) GJ_COL(4) GJ_COL(5) GJ_COL(6) GJ_COL(7) GJ_COL(8)
         default: break;
       }
       unsigned key = 0;
@@ -102,8 +102,8 @@ __device__ __noinline__ void gj_reg(double *A, int lda, int n, int *piv, const d
       const int br = 255 - (int)(key & 0xFFu);
       double cv = 0.0;
       switch (br >> 4) {
-        LU_PICK(0) LU_PICK(1) LU_PICK(2) LU_PICK(3) LU_PICK(4) LU_PICK(5) LU_PICK(6) LU_PICK(7)
-        LU_PICK(8)
+        GJ_PICK(0) GJ_PICK(1) GJ_PICK(2) GJ_PICK(3) GJ_PICK(4) GJ_PICK(5) GJ_PICK(6) GJ_PICK(7)
+        GJ_PICK(8)
         default: break;
       }
       const double pv = __shfl_sync(Z2_FULL, cv, hl | (br & 15));
@@ -131,7 +131,7 @@ __device__ __noinline__ void gj_reg(double *A, int lda, int n, int *piv, const d
 #pragma unroll
     for (int q = 0; q < S; ++q) rowv[q] = 0.0;
     switch (pr >> 4) {
-      LU_ROW(0) LU_ROW(1) LU_ROW(2) LU_ROW(3) LU_ROW(4) LU_ROW(5) LU_ROW(6) LU_ROW(7) LU_ROW(8)
+      GJ_ROW(0) GJ_ROW(1) GJ_ROW(2) GJ_ROW(3) GJ_ROW(4) GJ_ROW(5) GJ_ROW(6) GJ_ROW(7) GJ_ROW(8)
       default: break;
     }
     double u[S], l[S];
@@ -178,9 +178,9 @@ __device__ __noinline__ void gj_reg(double *A, int lda, int n, int *piv, const d
   __syncthreads();
 }
 
-#undef LU_COL
-#undef LU_ROW
-#undef LU_PICK
+#undef GJ_COL
+#undef GJ_ROW
+#undef GJ_PICK
 #undef GJ_PCOL
 
 // gj_reg for n <= 144 with work >= 4 n doubles; false when it does not apply.

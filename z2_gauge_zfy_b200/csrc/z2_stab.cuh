@@ -1,7 +1,7 @@
 // z2_stab.cuh -- UDV stabilization (src/stabilization.f90:42-200) on the
 // DMMA GEMM, the register-resident pivoted QR and the blocked DORGQR.
 #pragma once
-#include "z2_lu.cuh"
+#include "z2_gj.cuh"
 #include "z2_qrf.cuh"
 #include "z2_qrp.cuh"
 
@@ -190,7 +190,8 @@ __device__ __noinline__ void dev_stab_U_fast(const Smem &s, int N, double *A, in
 }
 
 // stab_green with the scale-split middle matrix; arguments as dev_stab_green
-// (W3 keeps the T factors of the QR's panels, W2 the right-hand side).
+// (W1 and W2 are N x N scratch; above N = 144, W3 keeps the T factors of the
+// QR's panels and W2 the right-hand side).
 __device__ __noinline__ void dev_stab_green_fast(const Smem &s, int N, int nt, int Ltrot,
                                                  const double *UR, const double *DR,
                                                  const double *VR, const double *ULT,
