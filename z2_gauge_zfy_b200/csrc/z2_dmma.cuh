@@ -777,55 +777,6 @@ __device__ __noinline__ void blk_inverse_blocked(double *A, int lda, int n, doub
   blk_copy(A, lda, W, ldw, n, n);
 }
 
-// Solve X R^T = Y in place (DTRSM 'R','U','T','N'): Y (nr x n, ldy) becomes
-// Y R^-T, R upper (ldr).  Column blocks of 8 from the right: the block's
-// columns are solved one thread per row (the 8 x 8 diagonal block of R in
-// registers; the same recurrence as blk_trsm_lun_blocked with a row of Y in
-// place of a column), then the columns to the left are updated by DMMA,
-// Y(:, 0:k0) -= Y(:, k0:k0+8) R(0:k0, k0:k0+8)^T.  Meant for a Y in shared
-// memory.
-__device__ __noinline__ void blk_trsm_rut_inplace(const double *R, int ldr, int n, double *Y,
-                                                  int ldy, int nr) {
-  const int last = ((n - 1) / 8) * 8;
-  for (int k0 = last; k0 >= 0; k0 -= 8) {
-    const int kb = (n - k0) < 8 ? (n - k0) : 8;
-    double rr[8][8];
-#pragma unroll
-    for (int p = 0; p < 8; ++p)
-#pragma unroll
-      for (int q = 0; q < 8; ++q)
-        rr[p][q] = (p <= q && q < kb) ? R[(k0 + p) + (size_t)(k0 + q) * ldr] : 0.0;
-    double rd[8];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) rd[q] = (q < kb) ? 1.0 / rr[q][q] : 0.0;
-    for (int i = threadIdx.x; i < nr; i += Z2_NT) {
-      double *Yi = Y + i + (size_t)k0 * ldy;
-      double y[8];
-#pragma unroll
-      for (int q = 0; q < 8; ++q) y[q] = (q < kb) ? Yi[(size_t)q * ldy] : 0.0;
-#pragma unroll
-      for (int q = 7; q >= 0; --q) {
-        if (q < kb) {
-          double z = y[q];
-          if (z != 0.0) {
-            z = z * rd[q];
-            y[q] = z;
-#pragma unroll
-            for (int p = 0; p < 8; ++p)
-              if (p < q) y[p] -= z * rr[p][q];
-          }
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < 8; ++q) if (q < kb) Yi[(size_t)q * ldy] = y[q];
-    }
-    __syncthreads();
-    if (k0 > 0)
-      blk_dmma(nr, k0, kb, -1.0, MatRef{Y + (size_t)k0 * ldy, 1, ldy}, false,
-               MatRef{R + (size_t)k0 * ldr, ldr, 1}, false, 1.0, Y, ldy);
-  }
-}
-
 // Solve R Z = Y in place (DTRSM 'L','U','N','N'), Y n x nc (ldy), R upper
 // (ldr).  Blocks of 8 rows from the bottom: the 8 x 8 diagonal block is
 // solved one thread per column (block of R held in registers), the rows
