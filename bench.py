@@ -494,7 +494,7 @@ def main():
         "flush_shape": ",".join(f"N{n}:{FLUSH_SHAPES[x]}" for n, x in sorted(smap.items())),
         "tuning": "z2_tune: ranks 4..64 (shared memory caps them: k <= 8 at N = 144) x every "
                   "flush tile shape valid for N, median SM cycles of 3 probe chains, first "
-                  "within 1.5 % of the fastest in the order (default shape, smaller rank)",
+                  "within 3 % of the fastest in the order (default shape, smaller rank)",
         "autotune_s": t_tune,
         "bin_observables_mean": dict(zip(("flux_avg", "chi_flux", "pair_sc_q0", "cdw_pi",
                                           "cdw_shift", "cdw_ratio", "density"),

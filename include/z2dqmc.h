@@ -195,7 +195,7 @@ int z2_tune_delay(const z2_chain_params *params, int32_t nchains, const z2_optio
  * Ltrot cut to 2*Nwrap; ranks 4..64 as z2_tune_delay, capped by shared memory,
  * times every flush shape valid for N) by the SM cycles of the chain kernel,
  * takes the median over the three probes, and picks, in the order (default
- * shape first, then smaller rank), the first candidate within 1.5 % of the
+ * shape first, then smaller rank), the first candidate within 3 % of the
  * fastest, so that repeated runs pick the same configuration.  k_out and
  * shape_out [nchains] are ready to pass as z2_options.delay_k_chain and
  * flush_shape_chain. */

@@ -1026,7 +1026,7 @@ static int probe_cycles(const std::vector<z2_chain_params> &probe, const z2_opti
 // lattice size: three probe chains per size (the chain's couplings and time
 // step, Ltrot cut to 2 Nwrap), every size side by side in one launch per
 // candidate, the median SM cycles of the three, and the first candidate in
-// preference order (default shape, then smaller rank) within 1.5 % of the
+// preference order (default shape, then smaller rank) within 3 % of the
 // fastest.
 static int tune_core(const z2_chain_params *params, int nchains, const z2_options *opt,
                      bool shapes, int32_t *k_out, int32_t *shape_out) {
@@ -1107,7 +1107,7 @@ static int tune_core(const z2_chain_params *params, int nchains, const z2_option
   for (int i = 0; i < ns; ++i) {
     const double best = *std::min_element(cost[i].begin(), cost[i].end());
     for (size_t ci = 0; ci < cands[i].size(); ++ci)
-      if (cost[i][ci] <= 1.015 * best) { pick[i] = cands[i][ci]; break; }
+      if (cost[i][ci] <= 1.03 * best) { pick[i] = cands[i][ci]; break; }
   }
   for (int c = 0; c < nchains; ++c) {
     const int N = params[c].Nlx * params[c].Nly;
